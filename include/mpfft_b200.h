@@ -1,0 +1,165 @@
+/*
+ * libmpfft_b200 -- B200 (sm_100a) implementation of mpFFT's conjugate-pair
+ * split-radix 2/4 DIT complex FFT, behind mpFFT's own C API.
+ *
+ * Two groups of entry points:
+ *
+ * 1. Drop-in replacements for the reference prototypes in mpFFT.h.  Same
+ *    names, argument meaning and out-of-place semantics; they return void as
+ *    the reference does and record a status readable with mpfft_last_error().
+ *    Only the top-level form is meaningful to an external caller (the
+ *    reference's own callers use (N,1,0,...), mpFFT.c:47,50): any power-of-two
+ *    n >= 1, any input stride s >= 1, sn >= 0 (element j read at in[j*s]).
+ *    A negative sn is the reference's internal wrap to its global N and is
+ *    rejected with MPFFT_EINVAL.  On any error the outputs are set to NaN.
+ *
+ * 2. An explicit plan/execute API with int status returns, batched execution
+ *    over many signals, device-resident limb planes (no mpfr_t conversion),
+ *    and scaled (1/N) output.
+ *
+ * Multiprecision numbers: the working precision P of a drop-in call is the
+ * largest precision among inr[0], ini[0], outr[0], outi[0]; each output
+ * element is rounded to nearest at its own precision (as MPFR rounds to the
+ * destination).  The device keeps one exponent per signal and fixed-point
+ * 32-bit limbs with P + log2(N) + 4 or more fraction bits; additions are
+ * exact and each twiddle product is rounded once, so the normwise error is
+ * below the reference's own at the same P.
+ *
+ * Thread safety: every entry point may be called from any host thread;
+ * calls on the same plan are serialised.
+ */
+#ifndef MPFFT_B200_H
+#define MPFFT_B200_H
+
+#include <stdint.h>
+
+#ifndef MPFFT_MPFR_TYPES_PROVIDED
+#include <mpfr.h>
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define MPFFT_OK 0
+#define MPFFT_EINVAL 1       /* bad argument (n not a power of two, s == 0, sn < 0, NULL, ...) */
+#define MPFFT_EUNSUPPORTED 2 /* valid but not supported by this build (e.g. precision too large for n) */
+#define MPFFT_ENONFINITE 3   /* NaN or infinity among the inputs */
+#define MPFFT_ECUDA 4        /* CUDA runtime error (no device, launch failure, ...) */
+#define MPFFT_ENOMEM 5       /* host or device allocation failed */
+
+/* flags */
+#define MPFFT_SCALED 1u         /* execute: multiply the result by 1/n (exact) */
+#define MPFFT_PLAN_HOST_ONLY 2u /* plan creation: conversion (pack/unpack) only, no device state */
+
+/* ------------------------------------------------------------------------ */
+/* 1. drop-in replacements for mpFFT.h                                      */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces mp_sr24_cp_fft, mpFFT.h:38,66 (implemented by
+ * lab/parallel/mp/parallel_mp_fft2.c:121-328 and
+ * lab/serial/mp/serial_mp_fft3.c:121-253). */
+void mp_sr24_cp_fft(unsigned long n, unsigned long s, long int sn, mpfr_t *inr, mpfr_t *ini, mpfr_t *outr,
+                    mpfr_t *outi);
+
+/* Replaces mp_sr24_cp_fft_v2, mpFFT.h:39 (lab/serial/mp/serial_mp_fft4.c:121-122):
+ * the pass-by-shift twiddle-index variant; log2n must be 0 at the top level. */
+void mp_sr24_cp_fft_v2(unsigned long n, unsigned long log2n, unsigned long s, long int sn, mpfr_t *inr,
+                       mpfr_t *ini, mpfr_t *outr, mpfr_t *outi);
+
+/* Scaled variant planned by the reference (README.md "unscaled and scaled"):
+ * out = FFT(in) / n.  The reference normalises with mpfr_div_ui(out,out,N)
+ * (lab/parallel/mp/parallel_mp_fft2.c:455); here the 1/n is an exact exponent
+ * shift applied before the single rounding into each output. */
+void mp_sr24_cp_fft_scaled(unsigned long n, unsigned long s, long int sn, mpfr_t *inr, mpfr_t *ini,
+                           mpfr_t *outr, mpfr_t *outi);
+
+/* Replaces d_sr24_cp_fft, mpFFT.h:25,53 (lab/serial/double/serial_d_fft6.c:93-429).
+ * Results are bit-identical to the reference's double transform. */
+void d_sr24_cp_fft(unsigned long n, unsigned long s, long int sn, double *inr, double *ini, double *outr,
+                   double *outi);
+
+/* Replaces d_sr24_cp_fft_v2, mpFFT.h:26 (lab/serial/double/serial_d_fft7.c:93-94). */
+void d_sr24_cp_fft_v2(unsigned long n, unsigned long log2n, unsigned long s, long int sn, double *inr,
+                      double *ini, double *outr, double *outi);
+
+/* FP64 scaled variant: out = FFT(in) * (1/n), exact power-of-two scaling. */
+void d_sr24_cp_fft_scaled(unsigned long n, unsigned long s, long int sn, double *inr, double *ini,
+                          double *outr, double *outi);
+
+/* Status of the last call made on this host thread (MPFFT_OK or an error
+ * code) and a human-readable message.  The reference has no error reporting
+ * (void returns, unchecked malloc); these are the drop-in's side channel. */
+int mpfft_last_error(void);
+const char *mpfft_last_error_string(void);
+
+/* ------------------------------------------------------------------------ */
+/* 2. explicit plan / execute API (no counterpart in the reference, which    */
+/*    has compile-time N and P and file-static twiddle tables, lut() in      */
+/*    lab/parallel/mp/parallel_mp_fft2.c:71-82)                              */
+/* ------------------------------------------------------------------------ */
+
+typedef struct mpfft_mp_plan mpfft_mp_plan;
+typedef struct mpfft_d_plan mpfft_d_plan;
+
+/* Plan a multiprecision transform of n points at working precision prec
+ * bits.  Builds the twiddle tables with MPFR and uploads them once. */
+int mpfft_mp_plan_create(mpfft_mp_plan **plan, unsigned long n, long prec);
+/* same, with flags (MPFFT_PLAN_HOST_ONLY: pack/unpack only, needs no GPU) */
+int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, long prec, unsigned flags);
+int mpfft_mp_plan_destroy(mpfft_mp_plan *plan);
+/* device format of a plan: limbs per real component, fraction bits */
+int mpfft_mp_plan_limbs(const mpfft_mp_plan *plan);
+long mpfft_mp_plan_frac_bits(const mpfft_mp_plan *plan);
+
+/* Transform `batch` signals held in host mpfr_t arrays: signal b occupies
+ * elements [b*n, (b+1)*n) of each array.  Synchronous. */
+int mpfft_mp_execute(mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr_t *ini, mpfr_t *outr,
+                     mpfr_t *outi, unsigned flags);
+
+/* Transform `batch` signals held on the device as limb planes: word
+ * (c, i, p, b) at base[((c*L + i)*n + p)*batch + b], c = 0 real / 1 imaginary,
+ * limb i < L (least significant first), two's complement.  in and out must
+ * not overlap.  Asynchronous on `stream` (a cudaStream_t, NULL = default). */
+int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, const uint32_t *d_in, uint32_t *d_out,
+                            void *stream);
+
+/* Host-side conversion between mpfr_t arrays and the limb-plane layout
+ * above.  exps[b] receives (pack) / supplies (unpack) the block exponent of
+ * signal b: a component with fixed-point integer A has value
+ * A * 2^(exps[b] - frac_bits).  unpack rounds to each output's precision. */
+int mpfft_mp_pack(const mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr_t *ini, uint32_t *planes,
+                  long *exps);
+int mpfft_mp_unpack(const mpfft_mp_plan *plan, unsigned long batch, const uint32_t *planes, const long *exps,
+                    mpfr_t *outr, mpfr_t *outi, unsigned flags);
+
+/* FP64 plans.  Host arrays: signal b at [b*n, (b+1)*n) of each array. */
+int mpfft_d_plan_create(mpfft_d_plan **plan, unsigned long n);
+int mpfft_d_plan_destroy(mpfft_d_plan *plan);
+int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const double *inr, const double *ini, double *outr,
+                    double *outi, unsigned flags);
+/* Device layout: word (c, p, b) at base[(c*n + p)*batch + b]. */
+int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, const double *d_in, double *d_out,
+                           unsigned flags, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* 3. diagnostics for benchmarks (no counterpart in the reference)          */
+/* ------------------------------------------------------------------------ */
+
+/* Breadth-first schedule of a plan: node size and node count of each
+ * butterfly launch (after the one leaf launch).  Returns the level count. */
+int mpfft_mp_plan_schedule(const mpfft_mp_plan *plan, int *level_n, int *level_nodes, int max_levels);
+/* mpfft_mp_execute_device with every launch bracketed by CUDA events on
+ * `stream`; launch_ms[0] = leaf launch, launch_ms[1+i] = level i.  Synchronous. */
+int mpfft_mp_execute_device_timed(mpfft_mp_plan *plan, unsigned long batch, const uint32_t *d_in,
+                                  uint32_t *d_out, void *stream, float *launch_ms);
+/* Measured integer multiply-add rate of the current GPU (ops/s): wide = 0 for
+ * 32-bit multiply-add, 1 for 32x32+64 -> 64-bit multiply-add. */
+int mpfft_diag_imad_rate(int wide, double *ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPFFT_B200_H */

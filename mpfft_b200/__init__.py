@@ -1,0 +1,220 @@
+"""mpfft_b200 -- B200-native conjugate-pair split-radix FFT behind mpFFT's C API.
+
+The product is the shared library ``libmpfft_b200.so`` (sm_100a kernels plus
+the C ABI declared in ``include/mpfft_b200.h``).  This module is a thin ctypes
+binding to it, mirroring the reference's entry points (``mpFFT.h``):
+
+* ``mp_sr24_cp_fft(n, s, sn, inr, ini, outr, outi)`` and friends take
+  addresses of ``mpfr_t`` arrays, exactly like the C functions;
+* ``MpPlan`` / ``DPlan`` expose the batched plan/execute API, including
+  device-resident execution on caller-owned CUDA buffers (e.g. torch tensors).
+
+There is no CPU fallback: if the library is missing, importing raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpfft_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "mpfft_b200.h")
+
+OK, EINVAL, EUNSUPPORTED, ENONFINITE, ECUDA, ENOMEM = 0, 1, 2, 3, 4, 5
+SCALED = 1
+PLAN_HOST_ONLY = 2
+
+
+class MpfftError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"mpfft error {code}: {msg}")
+        self.code = code
+
+
+def build(verbose: bool = False) -> None:
+    """Compile libmpfft_b200.so in-tree (nvcc, sm_100a)."""
+    out = None if verbose else subprocess.DEVNULL
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "csrc")], check=True, stdout=out)
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`"
+        )
+    L = C.CDLL(LIB_PATH)
+    vp, ul, sl, u32p, dp = C.c_void_p, C.c_ulong, C.c_long, C.c_void_p, C.c_void_p
+    sig = {
+        "mp_sr24_cp_fft": (None, [ul, ul, sl, vp, vp, vp, vp]),
+        "mp_sr24_cp_fft_v2": (None, [ul, ul, ul, sl, vp, vp, vp, vp]),
+        "mp_sr24_cp_fft_scaled": (None, [ul, ul, sl, vp, vp, vp, vp]),
+        "d_sr24_cp_fft": (None, [ul, ul, sl, dp, dp, dp, dp]),
+        "d_sr24_cp_fft_v2": (None, [ul, ul, ul, sl, dp, dp, dp, dp]),
+        "d_sr24_cp_fft_scaled": (None, [ul, ul, sl, dp, dp, dp, dp]),
+        "mpfft_last_error": (C.c_int, []),
+        "mpfft_last_error_string": (C.c_char_p, []),
+        "mpfft_mp_plan_create": (C.c_int, [C.POINTER(vp), ul, sl]),
+        "mpfft_mp_plan_create_flags": (C.c_int, [C.POINTER(vp), ul, sl, C.c_uint]),
+        "mpfft_mp_plan_destroy": (C.c_int, [vp]),
+        "mpfft_mp_plan_limbs": (C.c_int, [vp]),
+        "mpfft_mp_plan_frac_bits": (C.c_long, [vp]),
+        "mpfft_mp_execute": (C.c_int, [vp, ul, vp, vp, vp, vp, C.c_uint]),
+        "mpfft_mp_execute_device": (C.c_int, [vp, ul, u32p, u32p, vp]),
+        "mpfft_mp_pack": (C.c_int, [vp, ul, vp, vp, u32p, vp]),
+        "mpfft_mp_unpack": (C.c_int, [vp, ul, u32p, vp, vp, vp, C.c_uint]),
+        "mpfft_d_plan_create": (C.c_int, [C.POINTER(vp), ul]),
+        "mpfft_d_plan_destroy": (C.c_int, [vp]),
+        "mpfft_d_execute": (C.c_int, [vp, ul, dp, dp, dp, dp, C.c_uint]),
+        "mpfft_d_execute_device": (C.c_int, [vp, ul, dp, dp, C.c_uint, vp]),
+        "mpfft_mp_plan_schedule": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]),
+        "mpfft_mp_execute_device_timed": (C.c_int, [vp, ul, u32p, u32p, vp, C.POINTER(C.c_float)]),
+        "mpfft_diag_imad_rate": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+lib = _load()
+
+
+def header_functions() -> list[str]:
+    """Names of the functions declared in include/mpfft_b200.h."""
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(\w+)\s*\(", src, flags=re.M)))
+
+
+def last_error() -> tuple[int, str]:
+    return lib.mpfft_last_error(), (lib.mpfft_last_error_string() or b"").decode()
+
+
+def _check(code: int) -> None:
+    if code != OK:
+        raise MpfftError(code, last_error()[1])
+
+
+# ---------------------------------------------------------------------------
+# drop-in entry points (addresses of mpfr_t / double arrays)
+# ---------------------------------------------------------------------------
+
+def mp_sr24_cp_fft(n, s, sn, inr, ini, outr, outi) -> int:
+    lib.mp_sr24_cp_fft(n, s, sn, inr, ini, outr, outi)
+    return lib.mpfft_last_error()
+
+
+def mp_sr24_cp_fft_v2(n, log2n, s, sn, inr, ini, outr, outi) -> int:
+    lib.mp_sr24_cp_fft_v2(n, log2n, s, sn, inr, ini, outr, outi)
+    return lib.mpfft_last_error()
+
+
+def mp_sr24_cp_fft_scaled(n, s, sn, inr, ini, outr, outi) -> int:
+    lib.mp_sr24_cp_fft_scaled(n, s, sn, inr, ini, outr, outi)
+    return lib.mpfft_last_error()
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.c_void_p) if hasattr(a, "ctypes") else a
+
+
+def d_sr24_cp_fft(n, s, sn, inr, ini, outr, outi) -> int:
+    lib.d_sr24_cp_fft(n, s, sn, _dp(inr), _dp(ini), _dp(outr), _dp(outi))
+    return lib.mpfft_last_error()
+
+
+def d_sr24_cp_fft_v2(n, log2n, s, sn, inr, ini, outr, outi) -> int:
+    lib.d_sr24_cp_fft_v2(n, log2n, s, sn, _dp(inr), _dp(ini), _dp(outr), _dp(outi))
+    return lib.mpfft_last_error()
+
+
+def d_sr24_cp_fft_scaled(n, s, sn, inr, ini, outr, outi) -> int:
+    lib.d_sr24_cp_fft_scaled(n, s, sn, _dp(inr), _dp(ini), _dp(outr), _dp(outi))
+    return lib.mpfft_last_error()
+
+
+# ---------------------------------------------------------------------------
+# plans
+# ---------------------------------------------------------------------------
+
+class MpPlan:
+    """Multiprecision plan for n points at `prec` bits (device limb format)."""
+
+    def __init__(self, n: int, prec: int, host_only: bool = False):
+        h = C.c_void_p()
+        _check(lib.mpfft_mp_plan_create_flags(C.byref(h), n, prec, PLAN_HOST_ONLY if host_only else 0))
+        self.h = h
+        self.n, self.prec = n, prec
+        self.limbs = lib.mpfft_mp_plan_limbs(h)
+        self.frac_bits = lib.mpfft_mp_plan_frac_bits(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.mpfft_mp_plan_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def words(self, batch: int) -> int:
+        """32-bit words of one limb-plane buffer holding `batch` signals."""
+        return 2 * self.limbs * self.n * batch
+
+    def execute(self, batch, inr, ini, outr, outi, scaled=False) -> None:
+        _check(lib.mpfft_mp_execute(self.h, batch, inr, ini, outr, outi, SCALED if scaled else 0))
+
+    def execute_device(self, batch, d_in: int, d_out: int, stream: int = 0) -> None:
+        _check(lib.mpfft_mp_execute_device(self.h, batch, d_in, d_out, stream or None))
+
+    def schedule(self) -> list[tuple[int, int]]:
+        """[(node size n, node count)] of each butterfly launch after the leaf launch."""
+        a = (C.c_int * 32)()
+        b = (C.c_int * 32)()
+        k = lib.mpfft_mp_plan_schedule(self.h, a, b, 32)
+        return [(a[i], b[i]) for i in range(max(k, 0))]
+
+    def execute_device_timed(self, batch, d_in: int, d_out: int, stream: int = 0) -> list[float]:
+        """Per-launch durations (ms): [leaf, level 0, level 1, ...]."""
+        nl = len(self.schedule())
+        ms = (C.c_float * (nl + 1))()
+        _check(lib.mpfft_mp_execute_device_timed(self.h, batch, d_in, d_out, stream or None, ms))
+        return list(ms)
+
+    def pack(self, batch, inr, ini, planes_ptr: int, exps_ptr: int) -> None:
+        _check(lib.mpfft_mp_pack(self.h, batch, inr, ini, planes_ptr, exps_ptr))
+
+    def unpack(self, batch, planes_ptr, exps_ptr, outr, outi, scaled=False) -> None:
+        _check(lib.mpfft_mp_unpack(self.h, batch, planes_ptr, exps_ptr, outr, outi, SCALED if scaled else 0))
+
+
+def imad_rate(wide: bool = False) -> float:
+    """Measured integer multiply-add rate of the current GPU, ops/s."""
+    v = C.c_double()
+    _check(lib.mpfft_diag_imad_rate(1 if wide else 0, C.byref(v)))
+    return v.value
+
+
+class DPlan:
+    """FP64 plan for n points (bit-identical to the reference's double FFT)."""
+
+    def __init__(self, n: int):
+        h = C.c_void_p()
+        _check(lib.mpfft_d_plan_create(C.byref(h), n))
+        self.h = h
+        self.n = n
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.mpfft_d_plan_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def execute(self, batch, inr, ini, outr, outi, scaled=False) -> None:
+        _check(lib.mpfft_d_execute(self.h, batch, _dp(inr), _dp(ini), _dp(outr), _dp(outi),
+                                   SCALED if scaled else 0))
+
+    def execute_device(self, batch, d_in: int, d_out: int, scaled=False, stream: int = 0) -> None:
+        _check(lib.mpfft_d_execute_device(self.h, batch, d_in, d_out, SCALED if scaled else 0, stream or None))

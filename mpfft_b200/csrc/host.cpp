@@ -1,0 +1,802 @@
+// libmpfft_b200 host side: the C ABI declared in include/mpfft_b200.h.
+//
+// Responsibilities
+//  - plans: one per (n, limb count) for the mp tier and per n for FP64, cached
+//    process-wide; a plan owns the device twiddle tables, the breadth-first
+//    schedule of the split-radix tree, device buffers and a CUDA stream;
+//  - twiddles: built with MPFR at 32L+64 bits and rounded once to fixed point
+//    (the reference builds its LUT with MPFR at P, lut() in
+//    lab/parallel/mp/parallel_mp_fft2.c:71-82);
+//  - conversion between mpfr_t arrays and device limb planes (block floating
+//    point: one exponent per signal);
+//  - error status for the void drop-in entry points.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <functional>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "mpfr_abi.h"
+#define MPFFT_MPFR_TYPES_PROVIDED 1
+#include "../../include/mpfft_b200.h"
+#include "mpfft_internal.h"
+
+#define MPFFT_API extern "C" __attribute__((visibility("default")))
+
+namespace mpfft {
+
+// ---------------------------------------------------------------------------
+// status
+// ---------------------------------------------------------------------------
+static thread_local int g_err = MPFFT_OK;
+static thread_local char g_msg[256] = "";
+
+static int set_err(int code, const char *fmt, ...) {
+  g_err = code;
+  if (code == MPFFT_OK) {
+    g_msg[0] = 0;
+    return code;
+  }
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_msg, sizeof g_msg, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (expr);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return set_err(MPFFT_ECUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+static bool is_pow2(unsigned long n) { return n >= 1 && (n & (n - 1)) == 0; }
+static int ilog2(unsigned long n) {
+  int l = 0;
+  while ((1UL << l) < n) ++l;
+  return l;
+}
+
+// ---------------------------------------------------------------------------
+// breadth-first schedule of the reference's recursion tree
+// ---------------------------------------------------------------------------
+struct HostTree {
+  std::vector<Leaf> leaves;
+  std::map<int, std::vector<int>> levels;  // node size -> output offsets
+};
+
+// Walks the recursion of mp_sr24_cp_fft (parallel_mp_fft2.c:180-182):
+// (n/2, 2s, sn) -> out+0, (n/4, 4s, sn+s) -> out+n/2, (n/4, 4s, sn-s) -> out+3n/4.
+static void walk(HostTree &t, int n, int s, int sn, int out, int leaf_max) {
+  if (n <= leaf_max) {
+    t.leaves.push_back(Leaf{out, sn, s, n});
+    return;
+  }
+  walk(t, n / 2, 2 * s, sn, out, leaf_max);
+  walk(t, n / 4, 4 * s, sn + s, out + n / 2, leaf_max);
+  walk(t, n / 4, 4 * s, sn - s, out + 3 * n / 4, leaf_max);
+  t.levels[n].push_back(out);
+}
+
+struct DeviceTree {
+  TreeTables tabs;
+  Leaf *d_leaves = nullptr;
+  int *d_nodes = nullptr;
+  ~DeviceTree() {
+    if (d_leaves) cudaFree(d_leaves);
+    if (d_nodes) cudaFree(d_nodes);
+  }
+};
+
+static int build_tree(DeviceTree &dt, unsigned long N, int leaf_max) {
+  HostTree t;
+  walk(t, (int)N, 1, 0, 0, leaf_max);
+  dt.tabs.N = (int)N;
+  dt.tabs.nleaves = (int)t.leaves.size();
+  std::vector<int> nodes;
+  int lv = 0;
+  for (auto &kv : t.levels) {
+    if (lv >= kMaxLevels) return set_err(MPFFT_EUNSUPPORTED, "transform too large");
+    dt.tabs.level_n[lv] = kv.first;
+    dt.tabs.level_start[lv] = (int)nodes.size();
+    dt.tabs.level_count[lv] = (int)kv.second.size();
+    nodes.insert(nodes.end(), kv.second.begin(), kv.second.end());
+    ++lv;
+  }
+  dt.tabs.nlevels = lv;
+  CUDA_TRY(cudaMalloc(&dt.d_leaves, sizeof(Leaf) * t.leaves.size()));
+  CUDA_TRY(cudaMemcpy(dt.d_leaves, t.leaves.data(), sizeof(Leaf) * t.leaves.size(), cudaMemcpyHostToDevice));
+  if (!nodes.empty()) {
+    CUDA_TRY(cudaMalloc(&dt.d_nodes, sizeof(int) * nodes.size()));
+    CUDA_TRY(cudaMemcpy(dt.d_nodes, nodes.data(), sizeof(int) * nodes.size(), cudaMemcpyHostToDevice));
+  }
+  dt.tabs.leaves = dt.d_leaves;
+  dt.tabs.node_off = dt.d_nodes;
+  return MPFFT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fixed point <-> MPFR
+// ---------------------------------------------------------------------------
+
+// 32 bits of the non-negative integer M (32-bit words, least significant
+// first) starting at bit position pos (pos may be negative).
+static inline uint32_t bits32(const uint32_t *M, int nw, long pos) {
+  long w = pos >= 0 ? pos / 32 : -((-pos + 31) / 32);
+  int off = (int)(pos - w * 32);
+  uint64_t lo = (w >= 0 && w < nw) ? M[w] : 0;
+  uint64_t hi = (w + 1 >= 0 && w + 1 < nw) ? M[w + 1] : 0;
+  return (uint32_t)(((hi << 32) | lo) >> off);
+}
+
+// |x| * 2^(F - e_s), rounded to nearest (ties away), into L words; returns the
+// sign (0 / 1).  x must be a regular number or zero.
+static uint32_t mpfr_to_fixed(mpfr_srcptr x, int L, long F, long e_s, uint32_t *out) {
+  for (int i = 0; i < L; ++i) out[i] = 0;
+  if (mpfr_zero_p(x)) return 0;
+  const long prec = x->_mpfr_prec;
+  const int nl = (int)((prec + 63) / 64);
+  const uint32_t *M = reinterpret_cast<const uint32_t *>(x->_mpfr_d);  // little-endian 64-bit limbs
+  const int nw = 2 * nl;
+  // value = M * 2^(exp - 64 nl);  A = M * 2^sh
+  const long sh = (long)x->_mpfr_exp - 64L * nl + F - e_s;
+  for (int i = 0; i < L; ++i) out[i] = bits32(M, nw, 32L * i - sh);
+  if (sh < 0) {
+    const long rb = -sh - 1;  // highest discarded bit
+    uint32_t round_bit = (rb < 32L * nw) ? (bits32(M, nw, rb) & 1u) : 0u;
+    uint32_t c = round_bit;
+    for (int i = 0; i < L && c; ++i) {
+      uint64_t t = (uint64_t)out[i] + c;
+      out[i] = (uint32_t)t;
+      c = (uint32_t)(t >> 32);
+    }
+  }
+  return x->_mpfr_sign < 0 ? 1u : 0u;
+}
+
+// two's-complement L-word integer A -> y = A * 2^e2, rounded to y's precision.
+static void fixed_to_mpfr(const uint32_t *A, int L, long e2, mpfr_ptr y) {
+  uint32_t mag[80];
+  const bool neg = (A[L - 1] >> 31) != 0;
+  uint32_t c = neg ? 1u : 0u;
+  const uint32_t m = neg ? 0xffffffffu : 0u;
+  for (int i = 0; i < L; ++i) {
+    uint64_t t = (uint64_t)(A[i] ^ m) + c;
+    mag[i] = (uint32_t)t;
+    c = (uint32_t)(t >> 32);
+  }
+  int nw = L;
+  if (nw & 1) mag[nw++] = 0;
+  while (nw > 0 && mag[nw - 1] == 0) --nw;
+  if (nw == 0) {
+    mpfr_set_zero(y, 1);
+    return;
+  }
+  const int n64 = (nw + 1) / 2;
+  if (nw & 1) mag[nw] = 0;
+  __mpz_struct z;
+  z._mp_alloc = n64;
+  z._mp_size = neg ? -n64 : n64;
+  z._mp_d = reinterpret_cast<mp_limb_t *>(mag);
+  mpfr_set_z_2exp(y, &z, e2, MPFR_RNDN);
+}
+
+static void parallel_for(long n, long grain, const std::function<void(long, long)> &fn) {
+  unsigned hw = std::thread::hardware_concurrency();
+  long nthreads = std::min<long>(hw ? hw : 1, (n + grain - 1) / grain);
+  if (nthreads <= 1) {
+    fn(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  long chunk = (n + nthreads - 1) / nthreads;
+  for (long t = 0; t < nthreads; ++t) {
+    long a = t * chunk, b = std::min(n, a + chunk);
+    if (a >= b) break;
+    th.emplace_back([&fn, a, b] { fn(a, b); });
+  }
+  for (auto &x : th) x.join();
+}
+
+// ---------------------------------------------------------------------------
+// mp plans
+// ---------------------------------------------------------------------------
+
+// Limb count for (N, P): one sign bit, H = log2 N + 2 headroom bits and at
+// least P + log2 N + 4 fraction bits.
+static int mp_limbs_for(unsigned long N, long P) {
+  const long lg = ilog2(N);
+  long L = (P + 2 * lg + 7 + 31) / 32;
+  return (int)std::max<long>(L, kMinLimbs);
+}
+
+struct MpTwiddles {
+  uint32_t *d_tw = nullptr;
+  uint8_t *d_dneg = nullptr;
+  ~MpTwiddles() {
+    if (d_tw) cudaFree(d_tw);
+    if (d_dneg) cudaFree(d_dneg);
+  }
+};
+
+// Twiddle tables for (N, L): cos, cos+sin and |cos-sin| of 2 pi k/N, k < N/4,
+// as unsigned L-limb fixed-point with 32L-1 fraction bits, plus sign(cos-sin).
+static int build_twiddles(MpTwiddles &tw, unsigned long N, int L) {
+  const unsigned long q = N / 4;
+  if (q == 0) return MPFFT_OK;
+  std::vector<uint32_t> h((size_t)3 * L * q);
+  std::vector<uint8_t> neg(q);
+  const long pw = 32L * L + 64;
+  parallel_for((long)q, 16, [&](long a, long b) {
+    mpfr_t pi2, th, s, c, t;
+    mpfr_init2(pi2, pw + 32);
+    mpfr_init2(th, pw + 32);
+    mpfr_init2(s, pw);
+    mpfr_init2(c, pw);
+    mpfr_init2(t, pw);
+    mpfr_const_pi(pi2, MPFR_RNDN);
+    uint32_t tmp[80];
+    for (long k = a; k < b; ++k) {
+      mpfr_mul_ui(th, pi2, 2UL * (unsigned long)k, MPFR_RNDN);
+      mpfr_div_ui(th, th, N, MPFR_RNDN);
+      mpfr_sin_cos(s, c, th, MPFR_RNDN);
+      for (int which = 0; which < 3; ++which) {
+        if (which == 0) mpfr_set(t, c, MPFR_RNDN);
+        else if (which == 1) mpfr_add(t, c, s, MPFR_RNDN);
+        else mpfr_sub(t, c, s, MPFR_RNDN);
+        uint32_t sg = mpfr_to_fixed(t, L, 32L * L - 1, 0, tmp);
+        if (which == 2) neg[k] = (uint8_t)sg;
+        for (int i = 0; i < L; ++i) h[((size_t)which * L + i) * q + k] = tmp[i];
+      }
+    }
+    mpfr_clear(pi2);
+    mpfr_clear(th);
+    mpfr_clear(s);
+    mpfr_clear(c);
+    mpfr_clear(t);
+    mpfr_free_cache();
+  });
+  CUDA_TRY(cudaMalloc(&tw.d_tw, h.size() * sizeof(uint32_t)));
+  CUDA_TRY(cudaMemcpy(tw.d_tw, h.data(), h.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&tw.d_dneg, q));
+  CUDA_TRY(cudaMemcpy(tw.d_dneg, neg.data(), q, cudaMemcpyHostToDevice));
+  return MPFFT_OK;
+}
+
+}  // namespace mpfft
+
+using namespace mpfft;
+
+struct mpfft_mp_plan {
+  unsigned long N = 0;
+  long P = 0;
+  int L = 0;
+  long F = 0;  // fraction bits
+  bool host_only = false;  // conversion-only plan: no device state
+  DeviceTree tree;
+  MpTwiddles tw;
+  MpDeviceTables tabs;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  // staging for host-array execution, grown on demand
+  size_t cap_words = 0;
+  uint32_t *d_in = nullptr, *d_out = nullptr;
+  uint32_t *h_in = nullptr, *h_out = nullptr;
+  std::vector<long> exps;
+  ~mpfft_mp_plan() {
+    if (d_in) cudaFree(d_in);
+    if (d_out) cudaFree(d_out);
+    if (h_in) cudaFreeHost(h_in);
+    if (h_out) cudaFreeHost(h_out);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+struct mpfft_d_plan {
+  unsigned long N = 0;
+  DeviceTree tree;
+  double *d_wr = nullptr, *d_wi = nullptr;
+  DDeviceTables tabs;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  size_t cap = 0;
+  double *d_in = nullptr, *d_out = nullptr, *h_in = nullptr, *h_out = nullptr;
+  ~mpfft_d_plan() {
+    if (d_wr) cudaFree(d_wr);
+    if (d_wi) cudaFree(d_wi);
+    if (d_in) cudaFree(d_in);
+    if (d_out) cudaFree(d_out);
+    if (h_in) cudaFreeHost(h_in);
+    if (h_out) cudaFreeHost(h_out);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace mpfft {
+
+static int device_ready() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return set_err(MPFFT_ECUDA, "no CUDA device available: %s", cudaGetErrorString(e));
+  return MPFFT_OK;
+}
+
+static int mp_plan_init(mpfft_mp_plan *p, unsigned long n, long prec, bool host_only = false) {
+  if (!is_pow2(n)) return set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
+  if (prec < 2) return set_err(MPFFT_EINVAL, "precision %ld < 2", prec);
+  if (n > (1UL << 26)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
+  int L = mp_limbs_for(n, prec);
+  if (L > kMaxLimbs)
+    return set_err(MPFFT_EUNSUPPORTED, "precision %ld at n=%lu needs %d limbs (> %d supported)", prec, n, L,
+                   kMaxLimbs);
+  p->N = n;
+  p->P = prec;
+  p->L = L;
+  p->F = 32L * L - 1 - (ilog2(n) + 2);
+  p->host_only = host_only;
+  if (host_only) return MPFFT_OK;
+  if (int e = device_ready()) return e;
+  if (int e = build_tree(p->tree, n, 4)) return e;
+  if (int e = build_twiddles(p->tw, n, L)) return e;
+  static_cast<TreeTables &>(p->tabs) = p->tree.tabs;
+  p->tabs.tw = p->tw.d_tw;
+  p->tabs.dneg = p->tw.d_dneg;
+  CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  return MPFFT_OK;
+}
+
+// process-wide cache used by the drop-in entry points
+static std::mutex g_cache_mu;
+static std::map<std::pair<unsigned long, int>, std::unique_ptr<mpfft_mp_plan>> g_mp_cache;
+static std::map<unsigned long, std::unique_ptr<mpfft_d_plan>> g_d_cache;
+
+static mpfft_mp_plan *mp_cached(unsigned long n, long prec) {
+  std::lock_guard<std::mutex> g(g_cache_mu);
+  const int L = mp_limbs_for(n, prec);
+  auto key = std::make_pair(n, L);
+  auto it = g_mp_cache.find(key);
+  if (it != g_mp_cache.end()) return it->second.get();
+  std::unique_ptr<mpfft_mp_plan> p(new mpfft_mp_plan);
+  if (mp_plan_init(p.get(), n, prec) != MPFFT_OK) return nullptr;
+  auto *raw = p.get();
+  g_mp_cache[key] = std::move(p);
+  return raw;
+}
+
+static int mp_reserve(mpfft_mp_plan *p, unsigned long batch) {
+  const size_t words = (size_t)2 * p->L * p->N * batch;
+  if (words <= p->cap_words) return MPFFT_OK;
+  if (p->d_in) cudaFree(p->d_in);
+  if (p->d_out) cudaFree(p->d_out);
+  if (p->h_in) cudaFreeHost(p->h_in);
+  if (p->h_out) cudaFreeHost(p->h_out);
+  p->d_in = p->d_out = p->h_in = p->h_out = nullptr;
+  p->cap_words = 0;
+  if (cudaMalloc(&p->d_in, words * 4) != cudaSuccess || cudaMalloc(&p->d_out, words * 4) != cudaSuccess ||
+      cudaMallocHost(&p->h_in, words * 4) != cudaSuccess || cudaMallocHost(&p->h_out, words * 4) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(MPFFT_ENOMEM, "cannot allocate %zu-byte staging buffers", words * 4);
+  }
+  p->cap_words = words;
+  return MPFFT_OK;
+}
+
+// signal b, element p of a strided host array
+static inline mpfr_srcptr elem(mpfr_t *a, unsigned long b, unsigned long N, unsigned long p, unsigned long s) {
+  return a[b * N * s + p * s];
+}
+
+static int mp_pack_impl(const mpfft_mp_plan *P, unsigned long batch, mpfr_t *inr, mpfr_t *ini, unsigned long s,
+                        uint32_t *planes, long *exps) {
+  const unsigned long N = P->N;
+  const int L = P->L;
+  // block exponents and finiteness
+  std::vector<int> bad(batch, 0);
+  parallel_for((long)batch, 1, [&](long b0, long b1) {
+    for (long b = b0; b < b1; ++b) {
+      long e_s = LONG_MIN;
+      for (unsigned long p = 0; p < N; ++p) {
+        for (int c = 0; c < 2; ++c) {
+          mpfr_srcptr x = elem(c ? ini : inr, b, N, p, s);
+          if (!mpfr_number_p(x)) bad[b] = 1;
+          else if (!mpfr_zero_p(x) && x->_mpfr_exp > e_s) e_s = x->_mpfr_exp;
+        }
+      }
+      exps[b] = e_s == LONG_MIN ? 0 : e_s;
+    }
+  });
+  for (unsigned long b = 0; b < batch; ++b)
+    if (bad[b]) return set_err(MPFFT_ENONFINITE, "input signal %lu holds NaN or infinity", b);
+  const size_t plane = (size_t)N * batch;
+  parallel_for((long)(N * batch), 256, [&](long a0, long a1) {
+    uint32_t tmp[80];
+    for (long t = a0; t < a1; ++t) {
+      const unsigned long p = t / batch, b = t % batch;
+      for (int c = 0; c < 2; ++c) {
+        uint32_t sg = mpfr_to_fixed(elem(c ? ini : inr, b, N, p, s), L, P->F, exps[b], tmp);
+        if (sg) {  // two's complement
+          uint32_t cy = 1;
+          for (int i = 0; i < L; ++i) {
+            uint64_t v = (uint64_t)(uint32_t)~tmp[i] + cy;
+            tmp[i] = (uint32_t)v;
+            cy = (uint32_t)(v >> 32);
+          }
+        }
+        uint32_t *dst = planes + (size_t)c * L * plane + (size_t)p * batch + b;
+        for (int i = 0; i < L; ++i) dst[(size_t)i * plane] = tmp[i];
+      }
+    }
+  });
+  return MPFFT_OK;
+}
+
+static void mp_unpack_impl(const mpfft_mp_plan *P, unsigned long batch, const uint32_t *planes, const long *exps,
+                           mpfr_t *outr, mpfr_t *outi, unsigned flags) {
+  const unsigned long N = P->N;
+  const int L = P->L;
+  const size_t plane = (size_t)N * batch;
+  const long shift = (flags & MPFFT_SCALED) ? ilog2(N) : 0;
+  parallel_for((long)(N * batch), 256, [&](long a0, long a1) {
+    uint32_t tmp[80];
+    for (long t = a0; t < a1; ++t) {
+      const unsigned long p = t / batch, b = t % batch;
+      for (int c = 0; c < 2; ++c) {
+        const uint32_t *src = planes + (size_t)c * L * plane + (size_t)p * batch + b;
+        for (int i = 0; i < L; ++i) tmp[i] = src[(size_t)i * plane];
+        fixed_to_mpfr(tmp, L, exps[b] - P->F - shift, (c ? outi : outr)[b * N + p]);
+      }
+    }
+  });
+}
+
+static void mp_fill_nan(mpfr_t *a, unsigned long n) {
+  if (!a) return;
+  for (unsigned long k = 0; k < n; ++k) mpfr_set_nan(a[k]);
+}
+
+static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr, mpfr_t *ini, unsigned long s,
+                           mpfr_t *outr, mpfr_t *outi, unsigned flags) {
+  if (p->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
+  std::lock_guard<std::mutex> g(p->mu);
+  if (int e = mp_reserve(p, batch)) return e;
+  p->exps.assign(batch, 0);
+  if (int e = mp_pack_impl(p, batch, inr, ini, s, p->h_in, p->exps.data())) return e;
+  const size_t bytes = (size_t)2 * p->L * p->N * batch * 4;
+  CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, bytes, cudaMemcpyHostToDevice, p->stream));
+  CUDA_TRY(mp_run_transform(p->L, p->tabs, p->d_in, p->d_out, (int)batch, p->stream));
+  CUDA_TRY(cudaMemcpyAsync(p->h_out, p->d_out, bytes, cudaMemcpyDeviceToHost, p->stream));
+  CUDA_TRY(cudaStreamSynchronize(p->stream));
+  mp_unpack_impl(p, batch, p->h_out, p->exps.data(), outr, outi, flags);
+  return set_err(MPFFT_OK, "");
+}
+
+static long mp_call_prec(mpfr_t *inr, mpfr_t *ini, mpfr_t *outr, mpfr_t *outi) {
+  long P = mpfr_get_prec(outr[0]);
+  P = std::max<long>(P, mpfr_get_prec(outi[0]));
+  P = std::max<long>(P, mpfr_get_prec(inr[0]));
+  P = std::max<long>(P, mpfr_get_prec(ini[0]));
+  return P;
+}
+
+static void mp_dropin(unsigned long n, unsigned long s, long sn, mpfr_t *inr, mpfr_t *ini, mpfr_t *outr,
+                      mpfr_t *outi, unsigned flags) {
+  if (!inr || !ini || !outr || !outi) {
+    set_err(MPFFT_EINVAL, "NULL array");
+    return;
+  }
+  int e = MPFFT_OK;
+  if (!is_pow2(n)) e = set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
+  else if (s == 0) e = set_err(MPFFT_EINVAL, "stride s must be >= 1");
+  else if (sn < 0)
+    e = set_err(MPFFT_EINVAL, "sn=%ld < 0 addresses the reference's global array; only top-level calls (sn >= 0)", sn);
+  if (e == MPFFT_OK) {
+    mpfft_mp_plan *p = mp_cached(n, mp_call_prec(inr, ini, outr, outi));
+    if (!p) e = g_err;
+    else e = mp_execute_impl(p, 1, inr, ini, s, outr, outi, flags);
+  }
+  if (e != MPFFT_OK) {
+    mp_fill_nan(outr, n);
+    mp_fill_nan(outi, n);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 plans
+// ---------------------------------------------------------------------------
+static int d_plan_init(mpfft_d_plan *p, unsigned long n) {
+  if (!is_pow2(n)) return set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
+  if (n > (1UL << 28)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
+  if (int e = device_ready()) return e;
+  p->N = n;
+  if (int e = build_tree(p->tree, n, 16)) return e;
+  static_cast<TreeTables &>(p->tabs) = p->tree.tabs;
+  // twiddles exactly as the reference lut() (serial_d_fft6.c:52-62)
+  const unsigned long q = n / 4;
+  std::vector<double> wr(q ? q : 1), wi(q ? q : 1);
+  for (unsigned long k = 0; k < q; ++k) {
+    wr[k] = cos(2. * M_PI * k / n);
+    wi[k] = sin(2. * M_PI * k / n);
+  }
+  CUDA_TRY(cudaMalloc(&p->d_wr, wr.size() * sizeof(double)));
+  CUDA_TRY(cudaMalloc(&p->d_wi, wi.size() * sizeof(double)));
+  CUDA_TRY(cudaMemcpy(p->d_wr, wr.data(), wr.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(p->d_wi, wi.data(), wi.size() * sizeof(double), cudaMemcpyHostToDevice));
+  p->tabs.wr = p->d_wr;
+  p->tabs.wi = p->d_wi;
+  p->tabs.c8 = cos(2. * M_PI * 1 / 8);
+  p->tabs.c16a = cos(2. * M_PI * 1 / 16);
+  p->tabs.c16b = cos(2. * M_PI * 1 / 16) - cos(2. * M_PI * 3 / 16);
+  p->tabs.c16c = cos(2. * M_PI * 3 / 16);
+  p->tabs.c16d = cos(2. * M_PI * 1 / 16) + cos(2. * M_PI * 3 / 16);
+  CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  return MPFFT_OK;
+}
+
+static mpfft_d_plan *d_cached(unsigned long n) {
+  std::lock_guard<std::mutex> g(g_cache_mu);
+  auto it = g_d_cache.find(n);
+  if (it != g_d_cache.end()) return it->second.get();
+  std::unique_ptr<mpfft_d_plan> p(new mpfft_d_plan);
+  if (d_plan_init(p.get(), n) != MPFFT_OK) return nullptr;
+  auto *raw = p.get();
+  g_d_cache[n] = std::move(p);
+  return raw;
+}
+
+static int d_reserve(mpfft_d_plan *p, unsigned long batch) {
+  const size_t words = (size_t)2 * p->N * batch;
+  if (words <= p->cap) return MPFFT_OK;
+  if (p->d_in) cudaFree(p->d_in);
+  if (p->d_out) cudaFree(p->d_out);
+  if (p->h_in) cudaFreeHost(p->h_in);
+  if (p->h_out) cudaFreeHost(p->h_out);
+  p->d_in = p->d_out = p->h_in = p->h_out = nullptr;
+  p->cap = 0;
+  if (cudaMalloc(&p->d_in, words * 8) != cudaSuccess || cudaMalloc(&p->d_out, words * 8) != cudaSuccess ||
+      cudaMallocHost(&p->h_in, words * 8) != cudaSuccess || cudaMallocHost(&p->h_out, words * 8) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(MPFFT_ENOMEM, "cannot allocate %zu-byte staging buffers", words * 8);
+  }
+  p->cap = words;
+  return MPFFT_OK;
+}
+
+static double d_scale(const mpfft_d_plan *p, unsigned flags) {
+  return (flags & MPFFT_SCALED) ? 1.0 / (double)p->N : 1.0;
+}
+
+static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *inr, const double *ini,
+                          unsigned long s, double *outr, double *outi, unsigned flags) {
+  std::lock_guard<std::mutex> g(p->mu);
+  if (int e = d_reserve(p, batch)) return e;
+  const unsigned long N = p->N;
+  const size_t cim = (size_t)N * batch;
+  // [c][p][b] planes
+  for (unsigned long b = 0; b < batch; ++b)
+    for (unsigned long k = 0; k < N; ++k) {
+      p->h_in[k * batch + b] = inr[(b * N + k) * s];
+      p->h_in[cim + k * batch + b] = ini[(b * N + k) * s];
+    }
+  const size_t bytes = 2 * cim * sizeof(double);
+  CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, bytes, cudaMemcpyHostToDevice, p->stream));
+  CUDA_TRY(d_run_transform(p->tabs, p->d_in, p->d_out, (int)batch, d_scale(p, flags), p->stream));
+  CUDA_TRY(cudaMemcpyAsync(p->h_out, p->d_out, bytes, cudaMemcpyDeviceToHost, p->stream));
+  CUDA_TRY(cudaStreamSynchronize(p->stream));
+  for (unsigned long b = 0; b < batch; ++b)
+    for (unsigned long k = 0; k < N; ++k) {
+      outr[b * N + k] = p->h_out[k * batch + b];
+      outi[b * N + k] = p->h_out[cim + k * batch + b];
+    }
+  return set_err(MPFFT_OK, "");
+}
+
+static void d_dropin(unsigned long n, unsigned long s, long sn, double *inr, double *ini, double *outr,
+                     double *outi, unsigned flags) {
+  if (!inr || !ini || !outr || !outi) {
+    set_err(MPFFT_EINVAL, "NULL array");
+    return;
+  }
+  int e = MPFFT_OK;
+  if (!is_pow2(n)) e = set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
+  else if (s == 0) e = set_err(MPFFT_EINVAL, "stride s must be >= 1");
+  else if (sn < 0)
+    e = set_err(MPFFT_EINVAL, "sn=%ld < 0 addresses the reference's global array; only top-level calls (sn >= 0)", sn);
+  if (e == MPFFT_OK) {
+    mpfft_d_plan *p = d_cached(n);
+    if (!p) e = g_err;
+    else e = d_execute_impl(p, 1, inr, ini, s, outr, outi, flags);
+  }
+  if (e != MPFFT_OK && is_pow2(n)) {
+    for (unsigned long k = 0; k < n; ++k) outr[k] = outi[k] = NAN;
+  }
+}
+
+}  // namespace mpfft
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+MPFFT_API void mp_sr24_cp_fft(unsigned long n, unsigned long s, long sn, mpfr_t *inr, mpfr_t *ini, mpfr_t *outr,
+                              mpfr_t *outi) {
+  mp_dropin(n, s, sn, inr, ini, outr, outi, 0);
+}
+
+MPFFT_API void mp_sr24_cp_fft_v2(unsigned long n, unsigned long log2n, unsigned long s, long sn, mpfr_t *inr,
+                                 mpfr_t *ini, mpfr_t *outr, mpfr_t *outi) {
+  if (log2n != 0) {
+    set_err(MPFFT_EINVAL, "log2n=%lu != 0 is a sub-transform of the reference's global N", log2n);
+    if (is_pow2(n) && outr && outi) {
+      mp_fill_nan(outr, n);
+      mp_fill_nan(outi, n);
+    }
+    return;
+  }
+  mp_dropin(n, s, sn, inr, ini, outr, outi, 0);
+}
+
+MPFFT_API void mp_sr24_cp_fft_scaled(unsigned long n, unsigned long s, long sn, mpfr_t *inr, mpfr_t *ini,
+                                     mpfr_t *outr, mpfr_t *outi) {
+  mp_dropin(n, s, sn, inr, ini, outr, outi, MPFFT_SCALED);
+}
+
+MPFFT_API void d_sr24_cp_fft(unsigned long n, unsigned long s, long sn, double *inr, double *ini, double *outr,
+                             double *outi) {
+  d_dropin(n, s, sn, inr, ini, outr, outi, 0);
+}
+
+MPFFT_API void d_sr24_cp_fft_v2(unsigned long n, unsigned long log2n, unsigned long s, long sn, double *inr,
+                                double *ini, double *outr, double *outi) {
+  if (log2n != 0) {
+    set_err(MPFFT_EINVAL, "log2n=%lu != 0 is a sub-transform of the reference's global N", log2n);
+    if (is_pow2(n) && outr && outi)
+      for (unsigned long k = 0; k < n; ++k) outr[k] = outi[k] = NAN;
+    return;
+  }
+  d_dropin(n, s, sn, inr, ini, outr, outi, 0);
+}
+
+MPFFT_API void d_sr24_cp_fft_scaled(unsigned long n, unsigned long s, long sn, double *inr, double *ini,
+                                    double *outr, double *outi) {
+  d_dropin(n, s, sn, inr, ini, outr, outi, MPFFT_SCALED);
+}
+
+MPFFT_API int mpfft_last_error(void) { return g_err; }
+MPFFT_API const char *mpfft_last_error_string(void) { return g_msg; }
+
+MPFFT_API int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, long prec, unsigned flags) {
+  if (!plan) return set_err(MPFFT_EINVAL, "NULL plan pointer");
+  *plan = nullptr;
+  std::unique_ptr<mpfft_mp_plan> p(new (std::nothrow) mpfft_mp_plan);
+  if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
+  if (int e = mp_plan_init(p.get(), n, prec, (flags & MPFFT_PLAN_HOST_ONLY) != 0)) return e;
+  *plan = p.release();
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_mp_plan_create(mpfft_mp_plan **plan, unsigned long n, long prec) {
+  return mpfft_mp_plan_create_flags(plan, n, prec, 0);
+}
+
+MPFFT_API int mpfft_mp_plan_destroy(mpfft_mp_plan *plan) {
+  delete plan;
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_mp_plan_limbs(const mpfft_mp_plan *plan) { return plan ? plan->L : 0; }
+MPFFT_API long mpfft_mp_plan_frac_bits(const mpfft_mp_plan *plan) { return plan ? plan->F : 0; }
+
+MPFFT_API int mpfft_mp_execute(mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr_t *ini, mpfr_t *outr,
+                               mpfr_t *outi, unsigned flags) {
+  if (!plan || !inr || !ini || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  int e = mp_execute_impl(plan, batch, inr, ini, 1, outr, outi, flags);
+  if (e != MPFFT_OK) {
+    mp_fill_nan(outr, plan->N * batch);
+    mp_fill_nan(outi, plan->N * batch);
+  }
+  return e;
+}
+
+MPFFT_API int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, const uint32_t *d_in,
+                                      uint32_t *d_out, void *stream) {
+  if (!plan || !d_in || !d_out) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (plan->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  const size_t bytes = (size_t)2 * plan->L * plan->N * batch * 4;
+  const char *a = (const char *)d_in, *b = (const char *)d_out;
+  if (a < b + bytes && b < a + bytes) return set_err(MPFFT_EINVAL, "input and output buffers overlap");
+  if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream));
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_mp_pack(const mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr_t *ini,
+                            uint32_t *planes, long *exps) {
+  if (!plan || !inr || !ini || !planes || !exps) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (int e = mp_pack_impl(plan, batch, inr, ini, 1, planes, exps)) return e;
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_mp_unpack(const mpfft_mp_plan *plan, unsigned long batch, const uint32_t *planes,
+                              const long *exps, mpfr_t *outr, mpfr_t *outi, unsigned flags) {
+  if (!plan || !outr || !outi || !planes || !exps) return set_err(MPFFT_EINVAL, "NULL argument");
+  mp_unpack_impl(plan, batch, planes, exps, outr, outi, flags);
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_d_plan_create(mpfft_d_plan **plan, unsigned long n) {
+  if (!plan) return set_err(MPFFT_EINVAL, "NULL plan pointer");
+  *plan = nullptr;
+  std::unique_ptr<mpfft_d_plan> p(new (std::nothrow) mpfft_d_plan);
+  if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
+  if (int e = d_plan_init(p.get(), n)) return e;
+  *plan = p.release();
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_d_plan_destroy(mpfft_d_plan *plan) {
+  delete plan;
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const double *inr, const double *ini,
+                              double *outr, double *outi, unsigned flags) {
+  if (!plan || !inr || !ini || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  return d_execute_impl(plan, batch, inr, ini, 1, outr, outi, flags);
+}
+
+MPFFT_API int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, const double *d_in, double *d_out,
+                                     unsigned flags, void *stream) {
+  if (!plan || !d_in || !d_out) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  const size_t bytes = (size_t)2 * plan->N * batch * 8;
+  const char *a = (const char *)d_in, *b = (const char *)d_out;
+  if (a < b + bytes && b < a + bytes) return set_err(MPFFT_EINVAL, "input and output buffers overlap");
+  CUDA_TRY(d_run_transform(plan->tabs, d_in, d_out, (int)batch, d_scale(plan, flags), (cudaStream_t)stream));
+  return set_err(MPFFT_OK, "");
+}
+
+// ---------------------------------------------------------------------------
+// diagnostics for benchmarks
+// ---------------------------------------------------------------------------
+
+MPFFT_API int mpfft_mp_plan_schedule(const mpfft_mp_plan *plan, int *level_n, int *level_nodes, int max_levels) {
+  if (!plan || plan->host_only) return -1;
+  const int n = plan->tabs.nlevels;
+  for (int i = 0; i < n && i < max_levels; ++i) {
+    level_n[i] = plan->tabs.level_n[i];
+    level_nodes[i] = plan->tabs.level_count[i];
+  }
+  return n;
+}
+
+MPFFT_API int mpfft_mp_execute_device_timed(mpfft_mp_plan *plan, unsigned long batch, const uint32_t *d_in,
+                                            uint32_t *d_out, void *stream, float *launch_ms) {
+  if (!plan || !d_in || !d_out || !launch_ms) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (plan->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
+  CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream, launch_ms));
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_diag_imad_rate(int wide, double *ops_per_s) {
+  if (!ops_per_s) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (int e = device_ready()) return e;
+  CUDA_TRY(diag_imad_rate(wide, ops_per_s));
+  return set_err(MPFFT_OK, "");
+}

@@ -1,0 +1,315 @@
+// Multiprecision conjugate-pair split-radix 2/4 DIT FFT kernels (sm_100a).
+//
+// The reference computes the transform by depth-first recursion
+// (lab/parallel/mp/parallel_mp_fft2.c:121-328): a node of size n runs its
+// n/2 child on even samples, two n/4 children on samples 4m+1 and 4m-1 (the
+// conjugate pair), then one L-shaped butterfly per k in [0, n/4).  Here the
+// same tree is executed breadth-first: one launch runs every leaf (n = 4, 2 or
+// 1), then one launch per node size n = 8, 16, ..., N runs every butterfly of
+// every node of that size.  All nodes of one size are independent, so each
+// launch is one flat grid over (node, k, signal); consecutive threads are
+// consecutive signals of a batch (or consecutive k for a single signal),
+// which makes every limb-plane access a coalesced 128-byte transaction and,
+// for batches, makes the twiddle operand warp-uniform.
+//
+// Data layout (limb planes): word (c, i, p, b) of a batch of B signals of
+// N points, c = 0 real / 1 imaginary, limb i < L, at
+//   base[((c*L + i)*N + p)*B + b].
+#include <cstdint>
+
+#include "mp_limbs.cuh"
+#include "mpfft_internal.h"
+
+namespace mpfft {
+
+// ---------------------------------------------------------------------------
+// leaves: size-1, size-2 and size-4 DFTs of strided input subsequences
+// (reference base cases, parallel_mp_fft2.c:125-177).  Exact in fixed point.
+// ---------------------------------------------------------------------------
+template <int L>
+__global__ void __launch_bounds__(256) mp_leaf_kernel(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+                                                       int N, int B, const MpLeaf *__restrict__ leaves,
+                                                       int nleaves) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nleaves * B) return;
+  const int b = (int)(t % B);
+  const MpLeaf lf = leaves[t / B];
+  const size_t plane = (size_t)N * B;   // distance between limb planes
+  const size_t cim = (size_t)L * plane; // real -> imaginary component
+  // element j of the leaf's subsequence: index (sn + j*s), j=0 wrapped to sn+N
+  int idx[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) idx[j] = (j == 0 && lf.sn < 0) ? lf.sn + N : lf.sn + j * lf.s;
+  const uint32_t *x[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) x[j] = in + (size_t)(j < lf.n ? idx[j] : 0) * B + b;
+  uint32_t *y = out + (size_t)lf.out * B + b;
+  const size_t yB = B;
+
+  if (lf.n == 4) {
+    // X0 = x0+x2 + (x1+x3)      X2 = x0+x2 - (x1+x3)
+    // X1 = x0-x2 - i(x1-x3)     X3 = x0-x2 + i(x1-x3)
+    int64_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      const size_t o = i * plane;
+      int64_t r[4], m[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const uint32_t vr = x[j][o], vi = x[j][o + cim];
+        r[j] = (i == L - 1) ? (int64_t)(int32_t)vr : (int64_t)vr;
+        m[j] = (i == L - 1) ? (int64_t)(int32_t)vi : (int64_t)vi;
+      }
+      const int64_t er = r[0] + r[2], fr = r[0] - r[2], gr = r[1] + r[3], hr = r[1] - r[3];
+      const int64_t ei = m[0] + m[2], fi = m[0] - m[2], gi = m[1] + m[3], hi = m[1] - m[3];
+      const int64_t v[8] = {c[0] + er + gr, c[1] + fr + hi, c[2] + er - gr, c[3] + fr - hi,
+                            c[4] + ei + gi, c[5] + fi - hr, c[6] + ei - gi, c[7] + fi + hr};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        y[o + q * yB] = (uint32_t)v[q];
+        y[o + cim + q * yB] = (uint32_t)v[4 + q];
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) c[q] = v[q] >> 32;
+    }
+  } else if (lf.n == 2) {
+    int64_t c[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      const size_t o = i * plane;
+      int64_t r0 = x[0][o], r1 = x[1][o], i0 = x[0][o + cim], i1 = x[1][o + cim];
+      if (i == L - 1) {
+        r0 = (int32_t)r0; r1 = (int32_t)r1; i0 = (int32_t)i0; i1 = (int32_t)i1;
+      }
+      const int64_t v[4] = {c[0] + r0 + r1, c[1] + r0 - r1, c[2] + i0 + i1, c[3] + i0 - i1};
+      y[o] = (uint32_t)v[0];
+      y[o + yB] = (uint32_t)v[1];
+      y[o + cim] = (uint32_t)v[2];
+      y[o + cim + yB] = (uint32_t)v[3];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) c[q] = v[q] >> 32;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      const size_t o = i * plane;
+      y[o] = x[0][o];
+      y[o + cim] = x[0][o + cim];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// L-shaped combine of one butterfly (reference :238-252), streamed limb by
+// limb with signed 64-bit carries.  m1 = Z+ w^k and m2 = Z- w^-k sit in the
+// Z+ / Z- slots; when `swapped`, each slot holds (imag, real) instead of
+// (real, imag) -- the twiddle stage writes them that way to stay in place.
+// ---------------------------------------------------------------------------
+template <int L>
+__device__ __forceinline__ void combine(uint32_t *u0, uint32_t *u1, uint32_t *zp, uint32_t *zm, size_t plane,
+                                        size_t cim, bool swapped) {
+  const size_t sre = swapped ? cim : 0, sim = swapped ? 0 : cim;
+  int64_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int i = 0; i < L; ++i, u0 += plane, u1 += plane, zp += plane, zm += plane) {
+    const size_t o = 0;
+    const bool top = (i == L - 1);
+    auto s64 = [top](uint32_t v) -> int64_t { return top ? (int64_t)(int32_t)v : (int64_t)v; };
+    const int64_t a0r = s64(u0[o]), a0i = s64(u0[o + cim]);
+    const int64_t a1r = s64(u1[o]), a1i = s64(u1[o + cim]);
+    const int64_t pr = s64(zp[o + sre]), pi = s64(zp[o + sim]);
+    const int64_t mr = s64(zm[o + sre]), mi = s64(zm[o + sim]);
+    const int64_t sr = pr + mr, si = pi + mi, dr = pr - mr, di = pi - mi;
+    const int64_t v[8] = {c[0] + a0r + sr, c[1] + a0r - sr, c[2] + a1r + di, c[3] + a1r - di,
+                          c[4] + a0i + si, c[5] + a0i - si, c[6] + a1i - dr, c[7] + a1i + dr};
+    u0[o] = (uint32_t)v[0];
+    zp[o] = (uint32_t)v[1];
+    u1[o] = (uint32_t)v[2];
+    zm[o] = (uint32_t)v[3];
+    u0[o + cim] = (uint32_t)v[4];
+    zp[o + cim] = (uint32_t)v[5];
+    u1[o + cim] = (uint32_t)v[6];
+    zm[o + cim] = (uint32_t)v[7];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) c[q] = v[q] >> 32;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// one launch = every butterfly of every node of size n
+// ---------------------------------------------------------------------------
+//
+// Per butterfly k of a node at output offset `off` (q = n/4):
+//   U0 = y[off+k], U1 = y[off+k+q], Z+ = y[off+k+2q], Z- = y[off+k+3q]
+//   k = 0     : no twiddle (reference :184-201)
+//   k = q/2   : w^k = (1-i)/sqrt 2, four products by cos(pi/4) (:213-221)
+//   otherwise : 3 products per complex multiply with cos, cos+sin, cos-sin
+//               (3m3a, :222-236); twiddle index kn = k*(N/n) into the N/4 table.
+// The six products of a general butterfly run through one inlined product
+// routine in a rolled loop (one copy of the L^2/2 instruction block).
+template <int L>
+__global__ void __launch_bounds__(256) mp_level_kernel(uint32_t *__restrict__ y, int N, int B, int n,
+                                                        const int *__restrict__ node_off, int nnodes,
+                                                        const uint32_t *__restrict__ tw,
+                                                        const uint8_t *__restrict__ dneg) {
+  const int q = n >> 2;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nnodes * q * B) return;
+  const int b = (int)(t % B);
+  const long long r = t / B;
+  const int k = (int)(r % q);
+  const int off = node_off[r / q];
+  const size_t plane = (size_t)N * B;
+  const size_t cim = (size_t)L * plane;
+  uint32_t *u0 = y + (size_t)(off + k) * B + b;
+  uint32_t *u1 = u0 + (size_t)q * B;
+  uint32_t *zp = u0 + (size_t)2 * q * B;
+  uint32_t *zm = u0 + (size_t)3 * q * B;
+
+  if (k == 0) {
+    combine<L>(u0, u1, zp, zm, plane, cim, false);
+    return;
+  }
+  const int q4 = N >> 2;                 // twiddle table length
+  const size_t tplane = (size_t)q4;      // twiddle limb-plane stride
+  const int kn = k * (N / n);
+  const uint32_t *wr = tw + kn;                          // cos
+  const uint32_t *ws = tw + (size_t)L * tplane + kn;     // cos + sin
+  const uint32_t *wd = tw + (size_t)2 * L * tplane + kn; // cos - sin (signed)
+
+  uint32_t X[L], P[L];
+  if (2 * k == q) {
+    // side 0: m1r = (Zr+Zi)c -> Z+.im slot, m1i = (Zi-Zr)c -> Z+.re slot
+    // side 1: m2r = (Zr-Zi)c -> Z-.im slot, m2i = (Zr+Zi)c -> Z-.re slot
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+      uint32_t *zr = side ? zm : zp;
+      ld_addsub<L>(P, zr, zr + cim, plane, side == 1);
+      mul_tw<L>(P, wr, tplane, 0);
+      ld_addsub<L>(X, zr, zr + cim, plane, side == 0);
+      mul_tw<L>(X, wr, tplane, side == 0 ? 1u : 0u);
+      st<L>(zr + cim, plane, P);
+      st<L>(zr, plane, X);
+    }
+  } else {
+    const uint32_t dn = dneg[kn];
+    // step 0: P = (Zr +/- Zi) * cos
+    // step 1: X = Zi * (cos-sin), signed; m.r = P + X  -> Z.im slot
+    // step 2: X = Zr * (cos+sin);          m.i = +/-(P - X) -> Z.re slot
+    //   side 0 (Z+ w^k):  m1r = P - d*Zi, m1i = P - s*Zr   (P = (Zr+Zi)c)
+    //   side 1 (Z- w^-k): m2r = P + d*Zi, m2i = s*Zr - P   (P = (Zr-Zi)c)
+#pragma unroll 1
+    for (int st_ = 0; st_ < 6; ++st_) {
+      const int side = st_ >= 3;
+      const int step = st_ - 3 * side;
+      uint32_t *zr = side ? zm : zp;
+      uint32_t *zi = zr + cim;
+      const uint32_t *w;
+      uint32_t wn;
+      if (step == 0) {
+        ld_addsub<L>(X, zr, zi, plane, side == 1);
+        w = wr;
+        wn = 0;
+      } else if (step == 1) {
+        ld<L>(X, zi, plane);
+        w = wd;
+        wn = dn ^ (side == 0 ? 1u : 0u);
+      } else {
+        ld<L>(X, zr, plane);
+        w = ws;
+        wn = side == 0 ? 1u : 0u;
+      }
+      mul_tw<L>(X, w, tplane, wn);
+      if (step == 0) {
+#pragma unroll
+        for (int i = 0; i < L; ++i) P[i] = X[i];
+      } else if (step == 1) {
+        add<L>(X, X, P);
+        st<L>(zi, plane, X);
+      } else {
+        if (side == 0) add<L>(X, X, P);
+        else sub<L>(X, X, P);
+        st<L>(zr, plane, X);
+      }
+    }
+  }
+  combine<L>(u0, u1, zp, zm, plane, cim, true);
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers, one instantiation per supported limb count
+// ---------------------------------------------------------------------------
+
+// Optional per-launch timing with events on the launch stream.
+struct LaunchTimer {
+  float *ms;
+  cudaStream_t s;
+  cudaEvent_t ev[2 * (kMaxLevels + 1)] = {};
+  int n = 0;
+  LaunchTimer(float *ms_, cudaStream_t s_) : ms(ms_), s(s_) {}
+  void begin() {
+    if (!ms) return;
+    cudaEventCreate(&ev[2 * n]);
+    cudaEventCreate(&ev[2 * n + 1]);
+    cudaEventRecord(ev[2 * n], s);
+  }
+  void end() {
+    if (!ms) return;
+    cudaEventRecord(ev[2 * n + 1], s);
+    ++n;
+  }
+  ~LaunchTimer() {
+    if (!ms) return;
+    cudaStreamSynchronize(s);
+    for (int i = 0; i < n; ++i) {
+      cudaEventElapsedTime(&ms[i], ev[2 * i], ev[2 * i + 1]);
+      cudaEventDestroy(ev[2 * i]);
+      cudaEventDestroy(ev[2 * i + 1]);
+    }
+  }
+};
+
+template <int L>
+static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
+                                 cudaStream_t s, float *launch_ms) {
+  const int threads = 256;
+  LaunchTimer timer(launch_ms, s);
+  {
+    const long long total = (long long)T.nleaves * B;
+    const int blocks = (int)((total + threads - 1) / threads);
+    timer.begin();
+    mp_leaf_kernel<L><<<blocks, threads, 0, s>>>(in, out, T.N, B, T.leaves, T.nleaves);
+    timer.end();
+  }
+  for (int lv = 0; lv < T.nlevels; ++lv) {
+    const int n = T.level_n[lv];
+    const long long total = (long long)T.level_count[lv] * (n / 4) * B;
+    const int blocks = (int)((total + threads - 1) / threads);
+    timer.begin();
+    mp_level_kernel<L><<<blocks, threads, 0, s>>>(out, T.N, B, n, T.node_off + T.level_start[lv],
+                                                  T.level_count[lv], T.tw, T.dneg);
+    timer.end();
+  }
+  return cudaGetLastError();
+}
+
+#define MPFFT_MP_CASE(LL) \
+  case LL:                \
+    return run_transform<LL>(T, in, out, B, s, launch_ms);
+
+cudaError_t mp_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
+                             cudaStream_t s, float *launch_ms) {
+  switch (L) {
+    MPFFT_MP_CASE(2) MPFFT_MP_CASE(3) MPFFT_MP_CASE(4) MPFFT_MP_CASE(5) MPFFT_MP_CASE(6) MPFFT_MP_CASE(7)
+    MPFFT_MP_CASE(8) MPFFT_MP_CASE(9) MPFFT_MP_CASE(10) MPFFT_MP_CASE(11) MPFFT_MP_CASE(12)
+    MPFFT_MP_CASE(13) MPFFT_MP_CASE(14) MPFFT_MP_CASE(15) MPFFT_MP_CASE(16) MPFFT_MP_CASE(17)
+    MPFFT_MP_CASE(18) MPFFT_MP_CASE(19) MPFFT_MP_CASE(20) MPFFT_MP_CASE(21) MPFFT_MP_CASE(22)
+    MPFFT_MP_CASE(23) MPFFT_MP_CASE(24) MPFFT_MP_CASE(25) MPFFT_MP_CASE(26) MPFFT_MP_CASE(27)
+    MPFFT_MP_CASE(28) MPFFT_MP_CASE(29) MPFFT_MP_CASE(30) MPFFT_MP_CASE(31) MPFFT_MP_CASE(32)
+    MPFFT_MP_CASE(33) MPFFT_MP_CASE(34)
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace mpfft

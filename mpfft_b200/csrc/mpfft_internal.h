@@ -1,0 +1,63 @@
+// Internal declarations shared by the host library and the kernel files.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace mpfft {
+
+// One leaf of the split-radix tree (a node of size n <= 4 for the mp tier,
+// n <= 16 for the FP64 tier): its input elements are x[(sn + j*s)], j < n,
+// with the j = 0 element wrapped to sn + N when sn < 0, and its outputs go to
+// y[out .. out+n).
+struct Leaf {
+  int out;
+  int sn;
+  int s;
+  int n;
+};
+using MpLeaf = Leaf;
+
+constexpr int kMaxLevels = 32;
+
+// The breadth-first schedule of one transform size: every leaf, then for each
+// node size n = first_level_n .. N (doubling) the output offsets of all nodes
+// of that size.  Pointers are device pointers; the small arrays are host
+// copies of the per-level metadata.
+struct TreeTables {
+  int N = 0;
+  int nleaves = 0;
+  const Leaf *leaves = nullptr;
+  int nlevels = 0;
+  int level_n[kMaxLevels] = {};
+  int level_start[kMaxLevels] = {};
+  int level_count[kMaxLevels] = {};
+  const int *node_off = nullptr;
+};
+
+struct MpDeviceTables : TreeTables {
+  const uint32_t *tw = nullptr;   // [3][L][N/4]: cos, cos+sin, |cos-sin| magnitudes
+  const uint8_t *dneg = nullptr;  // [N/4]: sign of cos-sin
+};
+
+struct DDeviceTables : TreeTables {
+  const double *wr = nullptr;  // [N/4] cos(2 pi k/N)
+  const double *wi = nullptr;  // [N/4] sin(2 pi k/N)
+  double c8 = 0, c16a = 0, c16b = 0, c16c = 0, c16d = 0;
+};
+
+// largest limb count with register-resident kernels
+constexpr int kMaxLimbs = 34;
+constexpr int kMinLimbs = 2;
+
+// launch_ms (optional, host array of >= 1 + nlevels floats): when non-null,
+// each launch is bracketed by events on `s` and its duration written there
+// (the call then synchronizes); used by benchmarks to attribute time.
+cudaError_t mp_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
+                             cudaStream_t s, float *launch_ms = nullptr);
+cudaError_t diag_imad_rate(int wide, double *ops_per_s);
+cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
+                            cudaStream_t s);
+
+}  // namespace mpfft

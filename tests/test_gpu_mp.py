@@ -1,0 +1,197 @@
+"""GPU parity tests of the multiprecision path, through the C ABI.
+
+Acceptance: normwise relative error max_k max(|dRe|,|dIm|) / max_k |X_k|_inf
+against a direct MPFR DFT at 2P bits must be <= 8*log2(N)*2^-P, and no worse
+than the reference's own transform at the same P on the same inputs.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def M():
+    import mpfft_b200
+
+    return mpfft_b200
+
+
+def _inputs(O, n, p, seed, scale=0):
+    xr, xi = O.mp_pair(n, p)
+    O.fill_uniform(xr, xi, seed)
+    if scale:
+        O.lib().orc_mp_scale2(xr.ptr, n, scale)
+        O.lib().orc_mp_scale2(xi.ptr, n, scale)
+    return xr, xi
+
+
+def _gpu(M, O, xr, xi, n, p, fn="mp_sr24_cp_fft"):
+    yr, yi = O.mp_pair(n, p)
+    code = getattr(M, fn)(n, 1, 0, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
+    assert code == M.OK, M.last_error()
+    return yr, yi
+
+
+@pytest.mark.parametrize(
+    "n,p",
+    [(1, 64), (2, 64), (4, 64), (8, 64), (16, 64), (32, 128), (64, 256), (128, 53), (256, 1024), (512, 512),
+     (1024, 64), (1024, 256), (2048, 128)],
+)
+def test_mp_matches_2p_dft_oracle(M, orc, n, p):
+    O = orc
+    xr, xi = _inputs(O, n, p, 1000 + n)
+    yr, yi = _gpu(M, O, xr, xi, n, p)
+    dr, di = O.mp_pair(n, 2 * p)
+    O.mp_dft(xr, xi, dr, di)
+    e_gpu = O.mp_errors(yr, yi, dr, di)
+    bound = O.mp_bound_log2(n, p)
+    assert e_gpu["log2_rel"] <= bound, (e_gpu, bound)
+    # the reference's own transform on the same inputs, same P
+    rr, ri = O.mp_pair(n, p)
+    O.MpFFT(n, p)(xr, xi, rr, ri)
+    e_ref = O.mp_errors(rr, ri, dr, di)
+    assert e_gpu["log2_rel"] <= e_ref["log2_rel"] + 0.5, (e_gpu, e_ref)
+
+
+@pytest.mark.parametrize("g", load_golden("mp_"), ids=lambda g: g["name"])
+def test_mp_matches_reference_golden(M, orc, g):
+    O = orc
+    n, p = g["N"], g["P"]
+    xr, xi = O.mp_pair(n, p)
+    xr.set_hex(g["inr"])
+    xi.set_hex(g["ini"])
+    rr, ri = O.mp_pair(n, p)
+    rr.set_hex(g["outr"])
+    ri.set_hex(g["outi"])
+    yr, yi = _gpu(M, O, xr, xi, n, p)
+    e = O.mp_errors(yr, yi, rr, ri)
+    assert e["log2_rel"] <= O.mp_bound_log2(n, p), e
+
+
+def test_mp_v2_and_scaled(M, orc):
+    O = orc
+    n, p = 256, 192
+    xr, xi = _inputs(O, n, p, 7)
+    yr, yi = _gpu(M, O, xr, xi, n, p)
+    vr, vi = O.mp_pair(n, p)
+    assert M.mp_sr24_cp_fft_v2(n, 0, 1, 0, xr.ptr, xi.ptr, vr.ptr, vi.ptr) == M.OK
+    L = O.lib()
+    assert L.orc_mp_count_diff(yr.ptr, vr.ptr, n) == 0 and L.orc_mp_count_diff(yi.ptr, vi.ptr, n) == 0
+    sr, si = _gpu(M, O, xr, xi, n, p, fn="mp_sr24_cp_fft_scaled")
+    L.orc_mp_scale2(yr.ptr, n, -8)
+    L.orc_mp_scale2(yi.ptr, n, -8)
+    assert L.orc_mp_count_diff(yr.ptr, sr.ptr, n) == 0 and L.orc_mp_count_diff(yi.ptr, si.ptr, n) == 0
+
+
+def test_mp_batch_equals_single_calls(M, orc):
+    O = orc
+    n, p, batch = 128, 256, 5
+    xr, xi = O.mp_pair(n * batch, p)
+    O.fill_uniform(xr, xi, 31)
+    L = O.lib()
+    # make the signals differ in scale
+    for b, e in enumerate((0, 40, -40, 3, 0)):
+        for a in (xr, xi):
+            L.orc_mp_scale2(a.ptr + b * n * 32, n, e)
+    plan = M.MpPlan(n, p)
+    yr, yi = O.mp_pair(n * batch, p)
+    plan.execute(batch, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
+    for b in range(batch):
+        sr, si = O.mp_pair(n, p)
+        assert M.mp_sr24_cp_fft(n, 1, 0, xr.ptr + b * n * 32, xi.ptr + b * n * 32, sr.ptr, si.ptr) == M.OK
+        assert L.orc_mp_count_diff(sr.ptr, yr.ptr + b * n * 32, n) == 0
+        assert L.orc_mp_count_diff(si.ptr, yi.ptr + b * n * 32, n) == 0
+
+
+def test_mp_device_api_matches_host_api(M, orc):
+    import torch
+
+    O = orc
+    n, p, batch = 256, 128, 64
+    plan = M.MpPlan(n, p)
+    xr, xi = O.mp_pair(n * batch, p)
+    O.fill_uniform(xr, xi, 5)
+    host = np.zeros(plan.words(batch), dtype=np.uint32)
+    exps = np.zeros(batch, dtype=np.int64)
+    plan.pack(batch, xr.ptr, xi.ptr, host.ctypes.data, exps.ctypes.data)
+    d_in = torch.from_numpy(host.view(np.int32)).cuda()
+    d_out = torch.empty_like(d_in)
+    plan.execute_device(batch, d_in.data_ptr(), d_out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    out = d_out.cpu().numpy().view(np.uint32).copy()
+    yr, yi = O.mp_pair(n * batch, p)
+    plan.unpack(batch, out.ctypes.data, exps.ctypes.data, yr.ptr, yi.ptr)
+    zr, zi = O.mp_pair(n * batch, p)
+    plan.execute(batch, xr.ptr, xi.ptr, zr.ptr, zi.ptr)
+    L = O.lib()
+    assert L.orc_mp_count_diff(yr.ptr, zr.ptr, n * batch) == 0
+    assert L.orc_mp_count_diff(yi.ptr, zi.ptr, n * batch) == 0
+
+
+def test_mp_edge_inputs(M, orc):
+    O = orc
+    L = O.lib()
+    n, p = 64, 128
+    # all zero -> all zero
+    xr, xi = O.mp_pair(n, p)
+    yr, yi = _gpu(M, O, xr, xi, n, p)
+    assert np.all(yr.to_double() == 0) and np.all(yi.to_double() == 0)
+    # unit impulse at 0 -> all ones, exactly
+    L.orc_mp_set_ui(xr.ptr, 1, 1)
+    yr, yi = _gpu(M, O, xr, xi, n, p)
+    ones, zeros = O.mp_pair(n, p)
+    L.orc_mp_set_ui(ones.ptr, n, 1)
+    assert L.orc_mp_count_diff(yr.ptr, ones.ptr, n) == 0
+    assert L.orc_mp_count_diff(yi.ptr, zeros.ptr, n) == 0
+    # extreme block exponents: error relative to the signal's own scale
+    for sc in (40, -40, 1000, -1000):
+        xr, xi = _inputs(O, n, p, 3, scale=sc)
+        yr, yi = _gpu(M, O, xr, xi, n, p)
+        dr, di = O.mp_pair(n, 2 * p)
+        O.mp_dft(xr, xi, dr, di)
+        assert O.mp_errors(yr, yi, dr, di)["log2_rel"] <= O.mp_bound_log2(n, p)
+
+
+def test_mp_strided_input(M, orc):
+    O = orc
+    n, p, s = 128, 96, 3
+    xr, xi = O.mp_pair(n * s, p)
+    O.fill_uniform(xr, xi, 9)
+    yr, yi = O.mp_pair(n, p)
+    assert M.mp_sr24_cp_fft(n, s, 0, xr.ptr, xi.ptr, yr.ptr, yi.ptr) == M.OK
+    gr, gi = O.mp_pair(n, p)
+    O.lib().orc_mp_gather(gr.ptr, xr.ptr, n, s)
+    O.lib().orc_mp_gather(gi.ptr, xi.ptr, n, s)
+    zr, zi = _gpu(M, O, gr, gi, n, p)
+    L = O.lib()
+    assert L.orc_mp_count_diff(yr.ptr, zr.ptr, n) == 0 and L.orc_mp_count_diff(yi.ptr, zi.ptr, n) == 0
+
+
+def test_mp_nonfinite_input_reports_error(M, orc):
+    O = orc
+    n, p = 32, 64
+    xr, xi = _inputs(O, n, p, 1)
+    O.lib().orc_mp_set_inf(xr.ptr, 3, 1)
+    yr, yi = O.mp_pair(n, p)
+    assert M.mp_sr24_cp_fft(n, 1, 0, xr.ptr, xi.ptr, yr.ptr, yi.ptr) == M.ENONFINITE
+    assert np.all(np.isnan(yr.to_double()))
+
+
+@pytest.mark.parametrize("n,p", [(1 << 16, 256), (1 << 14, 1024)])
+def test_mp_large_n_roundtrip(M, orc, n, p):
+    """Size-independent property at full sizes: the inverse by the swap trick
+    (the reference's test(), parallel_mp_fft2.c:441-473) returns the input
+    within the error bound of two transforms."""
+    O = orc
+    xr, xi = _inputs(O, n, p, 17)
+    yr, yi = _gpu(M, O, xr, xi, n, p)
+    zr, zi = O.mp_pair(n, p)
+    assert M.mp_sr24_cp_fft_scaled(n, 1, 0, yi.ptr, yr.ptr, zr.ptr, zi.ptr) == M.OK
+    e = O.mp_errors(zi, zr, xr, xi)
+    assert e["log2_rel"] <= O.mp_bound_log2(n, p) + 1, e
