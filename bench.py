@@ -248,13 +248,21 @@ def main():
             dist.barrier()
 
     # ---- chosen (batched) form, device resident ----
-    for _ in range(args.warmup):
-        plan.execute_device(B, d_in.data_ptr(), d_out.data_ptr(), sh)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
+    # The clock sampler (200 ms period) starts with the warm-up, which runs
+    # for at least W steps and at least ~1 s, so samples cover the load that
+    # the timed steps run under.
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        t_w = time.perf_counter()
+        done = 0
+        while done < args.warmup or time.perf_counter() - t_w < 1.0:
+            plan.execute_device(B, d_in.data_ptr(), d_out.data_ptr(), sh)
+            done += 1
+            if done % 8 == 0:
+                torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(args.steps):
             plan.execute_device(B, d_in.data_ptr(), d_out.data_ptr(), sh)

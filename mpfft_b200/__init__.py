@@ -19,7 +19,8 @@ import re
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmpfft_b200.so")
+# MPFFT_B200_LIB may point at another build of the library (e.g. to compare builds)
+LIB_PATH = os.environ.get("MPFFT_B200_LIB") or os.path.join(HERE, "libmpfft_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "mpfft_b200.h")
 
 OK, EINVAL, EUNSUPPORTED, ENONFINITE, ECUDA, ENOMEM = 0, 1, 2, 3, 4, 5

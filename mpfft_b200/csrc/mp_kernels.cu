@@ -101,7 +101,8 @@ __global__ void __launch_bounds__(256) mp_leaf_kernel(const uint32_t *__restrict
 
 // ---------------------------------------------------------------------------
 // L-shaped combine of one butterfly (reference :238-252), streamed limb by
-// limb with signed 64-bit carries.  m1 = Z+ w^k and m2 = Z- w^-k sit in the
+// limb: a1 = m1 + m2, a2 = m1 - m2, then U0 +/- a1 and U1 -/+ i a2, twelve
+// independent modular carry chains.  m1 = Z+ w^k and m2 = Z- w^-k sit in the
 // Z+ / Z- slots; when `swapped`, each slot holds (imag, real) instead of
 // (real, imag) -- the twiddle stage writes them that way to stay in place.
 // ---------------------------------------------------------------------------
@@ -109,29 +110,23 @@ template <int L>
 __device__ __forceinline__ void combine(uint32_t *u0, uint32_t *u1, uint32_t *zp, uint32_t *zm, size_t plane,
                                         size_t cim, bool swapped) {
   const size_t sre = swapped ? cim : 0, sim = swapped ? 0 : cim;
-  int64_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // carry-in of each chain: 0 for additions, 1 for subtractions (a - b = a + ~b + 1)
+  uint32_t ca1r = 0, ca1i = 0, ca2r = 1, ca2i = 1;
+  uint32_t c0r = 0, c2r = 1, c1r = 0, c3r = 1, c0i = 0, c2i = 1, c1i = 1, c3i = 0;
 #pragma unroll
   for (int i = 0; i < L; ++i, u0 += plane, u1 += plane, zp += plane, zm += plane) {
-    const size_t o = 0;
-    const bool top = (i == L - 1);
-    auto s64 = [top](uint32_t v) -> int64_t { return top ? (int64_t)(int32_t)v : (int64_t)v; };
-    const int64_t a0r = s64(u0[o]), a0i = s64(u0[o + cim]);
-    const int64_t a1r = s64(u1[o]), a1i = s64(u1[o + cim]);
-    const int64_t pr = s64(zp[o + sre]), pi = s64(zp[o + sim]);
-    const int64_t mr = s64(zm[o + sre]), mi = s64(zm[o + sim]);
-    const int64_t sr = pr + mr, si = pi + mi, dr = pr - mr, di = pi - mi;
-    const int64_t v[8] = {c[0] + a0r + sr, c[1] + a0r - sr, c[2] + a1r + di, c[3] + a1r - di,
-                          c[4] + a0i + si, c[5] + a0i - si, c[6] + a1i - dr, c[7] + a1i + dr};
-    u0[o] = (uint32_t)v[0];
-    zp[o] = (uint32_t)v[1];
-    u1[o] = (uint32_t)v[2];
-    zm[o] = (uint32_t)v[3];
-    u0[o + cim] = (uint32_t)v[4];
-    zp[o + cim] = (uint32_t)v[5];
-    u1[o + cim] = (uint32_t)v[6];
-    zm[o + cim] = (uint32_t)v[7];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) c[q] = v[q] >> 32;
+    const uint32_t U0r = u0[0], U0i = u0[cim], U1r = u1[0], U1i = u1[cim];
+    const uint32_t m1r = zp[sre], m1i = zp[sim], m2r = zm[sre], m2i = zm[sim];
+    const uint32_t a1r = addc(m1r, m2r, ca1r), a1i = addc(m1i, m2i, ca1i);
+    const uint32_t a2r = addc(m1r, ~m2r, ca2r), a2i = addc(m1i, ~m2i, ca2i);
+    u0[0] = addc(U0r, a1r, c0r);
+    zp[0] = addc(U0r, ~a1r, c2r);
+    u1[0] = addc(U1r, a2i, c1r);
+    zm[0] = addc(U1r, ~a2i, c3r);
+    u0[cim] = addc(U0i, a1i, c0i);
+    zp[cim] = addc(U0i, ~a1i, c2i);
+    u1[cim] = addc(U1i, ~a2r, c1i);
+    zm[cim] = addc(U1i, a2r, c3i);
   }
 }
 
@@ -139,19 +134,32 @@ __device__ __forceinline__ void combine(uint32_t *u0, uint32_t *u1, uint32_t *zp
 // one launch = every butterfly of every node of size n
 // ---------------------------------------------------------------------------
 //
-// Per butterfly k of a node at output offset `off` (q = n/4):
+// Thread t handles signal b = t mod B of butterfly k of one node (q = n/4 at
+// output offset `off`):
 //   U0 = y[off+k], U1 = y[off+k+q], Z+ = y[off+k+2q], Z- = y[off+k+3q]
 //   k = 0     : no twiddle (reference :184-201)
-//   k = q/2   : w^k = (1-i)/sqrt 2, four products by cos(pi/4) (:213-221)
+//   k = q/2   : w^k = (1-i)/sqrt 2, products by cos(pi/4) (:213-221)
 //   otherwise : 3 products per complex multiply with cos, cos+sin, cos-sin
 //               (3m3a, :222-236); twiddle index kn = k*(N/n) into the N/4 table.
-// The six products of a general butterfly run through one inlined product
-// routine in a rolled loop (one copy of the L^2/2 instruction block).
+// For a batch that is a multiple of 32 every warp shares (node, k), so the
+// twiddle loads are warp-uniform broadcasts and no lane diverges.
+//
+// Both twiddled cases run as six steps of one rolled loop around a single
+// inlined product (one copy of its ~L^2 instructions keeps the instruction
+// cache warm).  Per side (Z+ then Z-), the step's operand, twiddle and the
+// rule that merges the product with P (the first product of the side, kept in
+// shared memory) are:
+//            step 0           step 1                      step 2
+//   general  P=(Zr+-Zi)c      m.r = P -+ d Zi -> im slot   m.i = +-(P - s Zr) -> re slot
+//   k = q/2  P=(Zr+-Zi)c      m.i = (Zi-Zr)c | (Zr+Zi)c    m.r = P -> im slot
+//                                   -> re slot
+// so m.r ends in the imaginary slot and m.i in the real slot ("swapped").
 template <int L>
-__global__ void __launch_bounds__(256) mp_level_kernel(uint32_t *__restrict__ y, int N, int B, int n,
-                                                        const int *__restrict__ node_off, int nnodes,
-                                                        const uint32_t *__restrict__ tw,
-                                                        const uint8_t *__restrict__ dneg) {
+__global__ void __launch_bounds__(128, 4) mp_level_kernel(uint32_t *__restrict__ y, int N, int B, int n,
+                                                          const int *__restrict__ node_off, int nnodes,
+                                                          const uint32_t *__restrict__ tw,
+                                                          const uint8_t *__restrict__ dneg) {
+  __shared__ uint32_t Ps[L * 128];
   const int q = n >> 2;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)nnodes * q * B) return;
@@ -170,67 +178,66 @@ __global__ void __launch_bounds__(256) mp_level_kernel(uint32_t *__restrict__ y,
     combine<L>(u0, u1, zp, zm, plane, cim, false);
     return;
   }
-  const int q4 = N >> 2;                 // twiddle table length
-  const size_t tplane = (size_t)q4;      // twiddle limb-plane stride
+  const size_t tplane = (size_t)(N >> 2);  // twiddle limb-plane stride
   const int kn = k * (N / n);
-  const uint32_t *wr = tw + kn;                          // cos
-  const uint32_t *ws = tw + (size_t)L * tplane + kn;     // cos + sin
-  const uint32_t *wd = tw + (size_t)2 * L * tplane + kn; // cos - sin (signed)
-
-  uint32_t X[L], P[L];
-  if (2 * k == q) {
-    // side 0: m1r = (Zr+Zi)c -> Z+.im slot, m1i = (Zi-Zr)c -> Z+.re slot
-    // side 1: m2r = (Zr-Zi)c -> Z-.im slot, m2i = (Zr+Zi)c -> Z-.re slot
+  const uint32_t *wr = tw + kn;                           // cos
+  const uint32_t *ws = tw + (size_t)L * tplane + kn;      // cos + sin
+  const uint32_t *wd = tw + (size_t)2 * L * tplane + kn;  // |cos - sin|
+  const bool special = (2 * k == q);
+  const bool dn = special ? false : (dneg[kn] != 0);
+  uint32_t *P = Ps + threadIdx.x;
+  const size_t ps = blockDim.x;
+  uint32_t X[L];
 #pragma unroll 1
-    for (int side = 0; side < 2; ++side) {
-      uint32_t *zr = side ? zm : zp;
-      ld_addsub<L>(P, zr, zr + cim, plane, side == 1);
-      mul_tw<L>(P, wr, tplane, 0);
-      ld_addsub<L>(X, zr, zr + cim, plane, side == 0);
-      mul_tw<L>(X, wr, tplane, side == 0 ? 1u : 0u);
-      st<L>(zr + cim, plane, P);
-      st<L>(zr, plane, X);
-    }
-  } else {
-    const uint32_t dn = dneg[kn];
-    // step 0: P = (Zr +/- Zi) * cos
-    // step 1: X = Zi * (cos-sin), signed; m.r = P + X  -> Z.im slot
-    // step 2: X = Zr * (cos+sin);          m.i = +/-(P - X) -> Z.re slot
-    //   side 0 (Z+ w^k):  m1r = P - d*Zi, m1i = P - s*Zr   (P = (Zr+Zi)c)
-    //   side 1 (Z- w^-k): m2r = P + d*Zi, m2i = s*Zr - P   (P = (Zr-Zi)c)
-#pragma unroll 1
-    for (int st_ = 0; st_ < 6; ++st_) {
-      const int side = st_ >= 3;
-      const int step = st_ - 3 * side;
-      uint32_t *zr = side ? zm : zp;
-      uint32_t *zi = zr + cim;
-      const uint32_t *w;
-      uint32_t wn;
-      if (step == 0) {
-        ld_addsub<L>(X, zr, zi, plane, side == 1);
-        w = wr;
-        wn = 0;
-      } else if (step == 1) {
-        ld<L>(X, zi, plane);
+  for (int st_ = 0; st_ < 6; ++st_) {
+    const int side = st_ >= 3;
+    const int step = st_ - 3 * side;
+    uint32_t *zr = side ? zm : zp;
+    uint32_t *zi = zr + cim;
+    const uint32_t *pa = zr, *pb = nullptr, *w = wr;
+    bool sub = false, negx = false, mul = true;
+    int sp = 0;
+    uint32_t *dst = nullptr;  // null: the product becomes P
+    if (step == 0) {
+      pb = zi;
+      sub = side;
+    } else if (!special) {
+      if (step == 1) {
+        pa = zi;
         w = wd;
-        wn = dn ^ (side == 0 ? 1u : 0u);
+        negx = dn ^ (side == 0);
+        sp = 1;
+        dst = zi;
       } else {
-        ld<L>(X, zr, plane);
         w = ws;
-        wn = side == 0 ? 1u : 0u;
+        negx = (side == 0);
+        sp = side ? -1 : 1;
+        dst = zr;
       }
-      mul_tw<L>(X, w, tplane, wn);
-      if (step == 0) {
-#pragma unroll
-        for (int i = 0; i < L; ++i) P[i] = X[i];
-      } else if (step == 1) {
-        add<L>(X, X, P);
-        st<L>(zi, plane, X);
+    } else {
+      if (step == 1) {
+        pa = side ? zr : zi;
+        pb = side ? zi : zr;
+        sub = !side;
+        dst = zr;
       } else {
-        if (side == 0) add<L>(X, X, P);
-        else sub<L>(X, X, P);
-        st<L>(zr, plane, X);
+        mul = false;
+        sp = 1;
+        dst = zi;
       }
+    }
+    if (mul) {
+      ld_addsub<L>(X, pa, pb, plane, sub);
+      mul_tw<L>(X, w, tplane);
+    } else {
+#pragma unroll
+      for (int i = 0; i < L; ++i) X[i] = 0;
+    }
+    if (!dst) {
+      st<L>(P, ps, X);
+    } else {
+      combine_p<L>(X, P, ps, negx, sp);
+      st<L>(dst, plane, X);
     }
   }
   combine<L>(u0, u1, zp, zm, plane, cim, true);
@@ -284,10 +291,11 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
   for (int lv = 0; lv < T.nlevels; ++lv) {
     const int n = T.level_n[lv];
     const long long total = (long long)T.level_count[lv] * (n / 4) * B;
-    const int blocks = (int)((total + threads - 1) / threads);
+    const int lthreads = 128;
+    const int blocks = (int)((total + lthreads - 1) / lthreads);
     timer.begin();
-    mp_level_kernel<L><<<blocks, threads, 0, s>>>(out, T.N, B, n, T.node_off + T.level_start[lv],
-                                                  T.level_count[lv], T.tw, T.dneg);
+    mp_level_kernel<L><<<blocks, lthreads, 0, s>>>(out, T.N, B, n, T.node_off + T.level_start[lv],
+                                                   T.level_count[lv], T.tw, T.dneg);
     timer.end();
   }
   return cudaGetLastError();

@@ -4,11 +4,12 @@
 // exponent per signal, kept on the host -- and each real component is an
 // L-limb two's-complement integer A (32-bit limbs, least significant first)
 // with F = 32L-1-H fraction bits, H = log2(N)+2 headroom bits.  Because the
-// format is fixed point, additions and subtractions are exact carry chains;
-// the only rounding in the whole transform is the one in each twiddle product.
+// format is fixed point, additions and subtractions are exact carry chains
+// (modular, so signs need no special handling); the only rounding in the whole
+// transform is the one in each twiddle product.
 //
 // Twiddles are unsigned L-limb magnitudes with 32L-1 fraction bits (|w| <= sqrt 2
-// for cos+sin), plus a sign that the caller supplies.
+// for cos+sin); their signs are applied by the caller when it combines products.
 //
 // Layout: limb i of a component lives at `ptr[i * plane]` -- limb planes, so
 // that consecutive threads (consecutive signals or butterfly indices) touch
@@ -19,9 +20,12 @@
 
 namespace mpfft {
 
-// ---------------------------------------------------------------------------
-// register-array load / store / add / sub
-// ---------------------------------------------------------------------------
+// one step of a carry chain: returns a + b + c (mod 2^32), c <- carry out
+__device__ __forceinline__ uint32_t addc(uint32_t a, uint32_t b, uint32_t &c) {
+  const uint64_t t = (uint64_t)a + b + c;
+  c = (uint32_t)(t >> 32);
+  return (uint32_t)t;
+}
 
 template <int L>
 __device__ __forceinline__ void ld(uint32_t (&x)[L], const uint32_t *p, size_t plane) {
@@ -35,77 +39,56 @@ __device__ __forceinline__ void st(uint32_t *p, size_t plane, const uint32_t (&x
   for (int i = 0; i < L; ++i, p += plane) *p = x[i];
 }
 
-// x = a + b (mod 2^(32L))
-template <int L>
-__device__ __forceinline__ void add(uint32_t (&x)[L], const uint32_t (&a)[L], const uint32_t (&b)[L]) {
-  uint32_t c = 0;
-#pragma unroll
-  for (int i = 0; i < L; ++i) {
-    uint64_t t = (uint64_t)a[i] + b[i] + c;
-    x[i] = (uint32_t)t;
-    c = (uint32_t)(t >> 32);
-  }
-}
-
-// x = a - b (mod 2^(32L))
-template <int L>
-__device__ __forceinline__ void sub(uint32_t (&x)[L], const uint32_t (&a)[L], const uint32_t (&b)[L]) {
-  uint32_t c = 1;  // a + ~b + 1
-#pragma unroll
-  for (int i = 0; i < L; ++i) {
-    uint64_t t = (uint64_t)a[i] + (uint32_t)~b[i] + c;
-    x[i] = (uint32_t)t;
-    c = (uint32_t)(t >> 32);
-  }
-}
-
-// x = pa + pb  or  pa - pb, streamed from memory
+// x = pa + pb  or  pa - pb, streamed from memory (pb may be null: x = pa)
 template <int L>
 __device__ __forceinline__ void ld_addsub(uint32_t (&x)[L], const uint32_t *pa, const uint32_t *pb,
                                           size_t plane, bool subtract) {
+  if (!pb) {
+    ld<L>(x, pa, plane);
+    return;
+  }
   const uint32_t m = subtract ? 0xffffffffu : 0u;
   uint32_t c = subtract ? 1u : 0u;
 #pragma unroll
-  for (int i = 0; i < L; ++i, pa += plane, pb += plane) {
-    uint64_t t = (uint64_t)*pa + (*pb ^ m) + c;
-    x[i] = (uint32_t)t;
-    c = (uint32_t)(t >> 32);
-  }
+  for (int i = 0; i < L; ++i, pa += plane, pb += plane) x[i] = addc(*pa, *pb ^ m, c);
 }
 
-// x = neg ? -x : x  (two's complement), branch free
+// x = sx*x + sp*p with sx in {+1,-1}, sp in {+1,-1,0}; p streamed from memory.
+// At most one operand is negated: a two's complement negation is ~v + 1.
 template <int L>
-__device__ __forceinline__ void cond_neg(uint32_t (&x)[L], uint32_t neg) {
-  const uint32_t m = 0u - neg;
-  uint32_t c = neg;
+__device__ __forceinline__ void combine_p(uint32_t (&x)[L], const uint32_t *p, size_t stride, bool negx,
+                                          int sp) {
+  const uint32_t mx = negx ? 0xffffffffu : 0u;
+  const uint32_t mp = sp < 0 ? 0xffffffffu : 0u;
+  const uint32_t keep = sp != 0 ? 0xffffffffu : 0u;
+  uint32_t c = (negx ? 1u : 0u) + (sp < 0 ? 1u : 0u);
 #pragma unroll
-  for (int i = 0; i < L; ++i) {
-    uint64_t t = (uint64_t)(x[i] ^ m) + c;
-    x[i] = (uint32_t)t;
-    c = (uint32_t)(t >> 32);
-  }
+  for (int i = 0; i < L; ++i, p += stride) x[i] = addc(x[i] ^ mx, (*p & keep) ^ mp, c);
 }
 
 // ---------------------------------------------------------------------------
-// truncated, rounded fixed-point product  x <- round(x * w / 2^(32L-1))
+// truncated, rounded signed fixed-point product  x <- round(x * w / 2^(32L-1))
 // ---------------------------------------------------------------------------
 //
-// In place: x holds the operand on entry and the product on return.
-// x: two's complement, |x| < 2^(32L-2).  w: unsigned magnitude (L limbs at
-// stride tplane), sign `wneg` (0/1).  Only partial products x_i*w_j with
-// i+j >= L-2 are formed (about L^2/2 + 3L/2 of them); the dropped lower part
-// is below L*2^-31 units of the result's last place.  Rounding is to nearest
-// (half-way cases away from zero, symmetric in sign).
+// In place: x (two's complement, |x| < 2^(32L-2)) holds the operand on entry
+// and the product on return.  w: unsigned magnitude, L limbs at stride tplane.
+//
+// The limbs of x are multiplied as an unsigned integer x_u = x + s*2^(32L)
+// (s = sign bit); the signed product is x_u*w - s*w*2^(32L), so for negative
+// x the twiddle is subtracted once from the columns at and above 32L.  Only
+// partial products x_i*w_j with i+j >= L-2 are formed (about L^2/2 + 3L/2 of
+// them); the dropped lower part is below L*2^-31 units of the result's last
+// place.  Adding 2^(32L-2) before the final shift rounds to nearest.
 //
 // The product is formed row by row (operand scanning): for each twiddle limb
-// w_j, the low halves of x_i*w_j are added with one carry chain and the high
-// halves with a second chain one column up.  Each partial product costs two
-// multiply-add instructions with carry.
+// w_j, one multiply-add-carry chain adds x_i*w_j into columns i+j.  Each step
+// is a 32x32+32+32 -> 64-bit multiply-add (it cannot overflow), written in
+// plain C so the compiler can schedule the two halves freely; on sm_100a this
+// issues faster than PTX mad.lo.cc/madc.hi.cc chains (measured).
 template <int L>
-__device__ __forceinline__ void mul_tw(uint32_t (&x)[L], const uint32_t *w, size_t tplane, uint32_t wneg) {
+__device__ __forceinline__ void mul_tw(uint32_t (&x)[L], const uint32_t *w, size_t tplane) {
   static_assert(L >= 2, "fixed-point product needs at least two limbs");
-  const uint32_t xneg = x[L - 1] >> 31;
-  cond_neg<L>(x, xneg);
+  const uint32_t smask = 0u - (x[L - 1] >> 31);
 
   // acc[a] holds column (L-2+a), a = 0 .. L+1
   uint32_t acc[L + 2];
@@ -113,28 +96,29 @@ __device__ __forceinline__ void mul_tw(uint32_t (&x)[L], const uint32_t *w, size
   for (int a = 0; a < L + 2; ++a) acc[a] = 0;
   acc[1] = 1u << 30;  // + 2^(32L-2): round to nearest on the final >> (32L-1)
 
+  const uint32_t *w0 = w;
 #pragma unroll
   for (int j = 0; j < L; ++j, w += tplane) {
     const uint32_t t = *w;
     const int i0 = (L - 2 - j) > 0 ? (L - 2 - j) : 0;
-    // low halves: columns i0+j .. L-1+j  ->  acc[i0+j-(L-2)] .. acc[j+1], carry into acc[j+2]
-    asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(acc[i0 + j - (L - 2)]) : "r"(x[i0]), "r"(t));
+    uint32_t c = 0;
 #pragma unroll
-    for (int i = i0 + 1; i < L; ++i)
-      asm volatile("madc.lo.cc.u32 %0, %1, %2, %0;" : "+r"(acc[i + j - (L - 2)]) : "r"(x[i]), "r"(t));
-    asm volatile("addc.u32 %0, %0, 0;" : "+r"(acc[j + 2]));
-    // high halves: columns i0+j+1 .. L+j  ->  acc[i0+j+1-(L-2)] .. acc[j+2], carry into acc[j+3]
-    asm volatile("mad.hi.cc.u32 %0, %1, %2, %0;" : "+r"(acc[i0 + j + 1 - (L - 2)]) : "r"(x[i0]), "r"(t));
-#pragma unroll
-    for (int i = i0 + 1; i < L; ++i)
-      asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(acc[i + j + 1 - (L - 2)]) : "r"(x[i]), "r"(t));
-    if (j + 3 <= L + 1)  // the last row's high chain cannot carry out (product < 2^(64L))
-      asm volatile("addc.u32 %0, %0, 0;" : "+r"(acc[(j + 3 <= L + 1) ? j + 3 : L + 1]));
+    for (int i = i0; i < L; ++i) {
+      const uint64_t pr = (uint64_t)x[i] * t + acc[i + j - (L - 2)] + c;
+      acc[i + j - (L - 2)] = (uint32_t)pr;
+      c = (uint32_t)(pr >> 32);
+    }
+    acc[j + 2] = c;  // column L+j is still empty: rows < j reach column L+j-1
   }
-  // r = (columns L-1 .. 2L-1) >> 31
+  // signed correction: acc -= s * w * 2^(32L)  (columns L .. 2L-1 = acc[2 .. L+1])
+  {
+    uint32_t c = 1;
+#pragma unroll
+    for (int j = 0; j < L; ++j, w0 += tplane) acc[j + 2] = addc(acc[j + 2], ~(*w0 & smask), c);
+  }
+  // x = (columns L-1 .. 2L-1) >> 31
 #pragma unroll
   for (int i = 0; i < L; ++i) x[i] = __funnelshift_r(acc[i + 1], acc[i + 2], 31);
-  cond_neg<L>(x, xneg ^ wneg);
 }
 
 }  // namespace mpfft

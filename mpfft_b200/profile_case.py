@@ -1,0 +1,60 @@
+"""Run the device-resident multiprecision transform on synthetic limb planes.
+
+A small, self-contained driver for profilers (ncu) and quick timing:
+
+    python -m mpfft_b200.profile_case --n 1024 --prec 1024 --batch 512 --reps 2
+
+The input planes are random two's-complement fixed-point values of magnitude
+below 2^F (F = the plan's fraction bits), i.e. a block-normalised signal with
+components in (-1, 1): exactly what packing uniform [-1,1) mpfr_t inputs
+produces.  Prints per-launch milliseconds of the last repetition.
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+
+
+def synthetic_planes(n: int, limbs: int, frac_bits: int, batch: int, seed: int = 1) -> np.ndarray:
+    """Limb planes [c][i][p][b] of uniform values in (-1, 1) * 2^F."""
+    rng = np.random.default_rng(seed)
+    words = rng.integers(0, 2**32, size=(2, limbs, n, batch), dtype=np.uint64).astype(np.uint32)
+    top_bits = frac_bits - 32 * (limbs - 1)  # bits of the magnitude in the top limb
+    top = words[:, limbs - 1].astype(np.int64) & ((1 << top_bits) - 1)
+    neg = rng.integers(0, 2, size=top.shape, dtype=np.int64).astype(bool)
+    # two's complement negation of the whole number is not needed for a valid
+    # input: any integer with |A| < 2^F is valid; set the sign by the top limb
+    top = np.where(neg, top - (1 << top_bits), top)
+    words[:, limbs - 1] = (top & 0xFFFFFFFF).astype(np.uint32)
+    return words.reshape(-1)
+
+
+def main():
+    import torch
+
+    import mpfft_b200 as M
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=1024)
+    ap.add_argument("--prec", type=int, default=1024)
+    ap.add_argument("--batch", type=int, default=512)
+    ap.add_argument("--reps", type=int, default=2)
+    a = ap.parse_args()
+    plan = M.MpPlan(a.n, a.prec)
+    host = synthetic_planes(a.n, plan.limbs, plan.frac_bits, a.batch)
+    d_in = torch.from_numpy(host.view(np.int32)).cuda()
+    d_out = torch.empty_like(d_in)
+    s = torch.cuda.current_stream().cuda_stream
+    ms = None
+    for _ in range(a.reps):
+        ms = plan.execute_device_timed(a.batch, d_in.data_ptr(), d_out.data_ptr(), s)
+    torch.cuda.synchronize()
+    sched = plan.schedule()
+    print(f"n={a.n} prec={a.prec} limbs={plan.limbs} batch={a.batch} total={sum(ms):.3f} ms "
+          f"({a.batch / sum(ms) * 1e3:.0f} FFT/s)")
+    print("leaf", round(ms[0], 4), " ".join(f"n{nn}:{t:.4f}" for (nn, _), t in zip(sched, ms[1:])))
+
+
+if __name__ == "__main__":
+    main()

@@ -89,14 +89,17 @@ def test_mp_v2_and_scaled(M, orc):
     assert L.orc_mp_count_diff(yr.ptr, sr.ptr, n) == 0 and L.orc_mp_count_diff(yi.ptr, si.ptr, n) == 0
 
 
-def test_mp_batch_equals_single_calls(M, orc):
+@pytest.mark.parametrize("n,p,batch", [(128, 256, 5), (128, 1024, 32), (64, 100, 64)])
+def test_mp_batch_equals_single_calls(M, orc, n, p, batch):
+    """Batches that are a multiple of 32 run the warp-per-butterfly kernel,
+    others and single signals the thread-per-butterfly kernel: all bit-equal."""
     O = orc
-    n, p, batch = 128, 256, 5
     xr, xi = O.mp_pair(n * batch, p)
     O.fill_uniform(xr, xi, 31)
     L = O.lib()
     # make the signals differ in scale
-    for b, e in enumerate((0, 40, -40, 3, 0)):
+    for b in range(batch):
+        e = (0, 40, -40, 3, 0)[b % 5]
         for a in (xr, xi):
             L.orc_mp_scale2(a.ptr + b * n * 32, n, e)
     plan = M.MpPlan(n, p)
