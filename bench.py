@@ -49,7 +49,7 @@ def parse_args():
     ap.add_argument("--impl", default="mpfft", choices=["mpfft", "reference"])
     ap.add_argument("--n", type=int, default=1024)
     ap.add_argument("--prec", type=int, default=1024)
-    ap.add_argument("--batch", type=int, default=512, help="signals per GPU per step")
+    ap.add_argument("--batch", type=int, default=2048, help="signals per GPU per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-accuracy", action="store_true")
     return ap.parse_args()

@@ -52,6 +52,7 @@ extern "C" {
 /* flags */
 #define MPFFT_SCALED 1u         /* execute: multiply the result by 1/n (exact) */
 #define MPFFT_PLAN_HOST_ONLY 2u /* plan creation: conversion (pack/unpack) only, no device state */
+#define MPFFT_PLAN_HOST_CONVERSION 4u /* plan creation: convert mpfr_t <-> limbs on the host, not the GPU */
 
 /* ------------------------------------------------------------------------ */
 /* 1. drop-in replacements for mpFFT.h                                      */
@@ -114,7 +115,10 @@ int mpfft_mp_plan_limbs(const mpfft_mp_plan *plan);
 long mpfft_mp_plan_frac_bits(const mpfft_mp_plan *plan);
 
 /* Transform `batch` signals held in host mpfr_t arrays: signal b occupies
- * elements [b*n, (b+1)*n) of each array.  Synchronous. */
+ * elements [b*n, (b+1)*n) of each array.  Synchronous.  When every input has
+ * the same number of significand limbs and every output the same precision,
+ * the conversion to and from limb planes runs on the GPU (the host only copies
+ * significand limbs); otherwise on the host.  Both give identical results. */
 int mpfft_mp_execute(mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr_t *ini, mpfr_t *outr,
                      mpfr_t *outi, unsigned flags);
 

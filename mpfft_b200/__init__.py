@@ -26,6 +26,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "mpfft_b200.h")
 OK, EINVAL, EUNSUPPORTED, ENONFINITE, ECUDA, ENOMEM = 0, 1, 2, 3, 4, 5
 SCALED = 1
 PLAN_HOST_ONLY = 2
+PLAN_HOST_CONVERSION = 4
 
 
 class MpfftError(RuntimeError):
@@ -144,9 +145,10 @@ def d_sr24_cp_fft_scaled(n, s, sn, inr, ini, outr, outi) -> int:
 class MpPlan:
     """Multiprecision plan for n points at `prec` bits (device limb format)."""
 
-    def __init__(self, n: int, prec: int, host_only: bool = False):
+    def __init__(self, n: int, prec: int, host_only: bool = False, host_conversion: bool = False):
         h = C.c_void_p()
-        _check(lib.mpfft_mp_plan_create_flags(C.byref(h), n, prec, PLAN_HOST_ONLY if host_only else 0))
+        flags = (PLAN_HOST_ONLY if host_only else 0) | (PLAN_HOST_CONVERSION if host_conversion else 0)
+        _check(lib.mpfft_mp_plan_create_flags(C.byref(h), n, prec, flags))
         self.h = h
         self.n, self.prec = n, prec
         self.limbs = lib.mpfft_mp_plan_limbs(h)

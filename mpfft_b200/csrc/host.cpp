@@ -286,6 +286,7 @@ struct mpfft_mp_plan {
   int L = 0;
   long F = 0;  // fraction bits
   bool host_only = false;  // conversion-only plan: no device state
+  bool force_host_conversion = false;  // convert mpfr_t <-> limbs on the host even when the GPU could
   DeviceTree tree;
   MpTwiddles tw;
   MpDeviceTables tabs;
@@ -296,7 +297,34 @@ struct mpfft_mp_plan {
   uint32_t *d_in = nullptr, *d_out = nullptr;
   uint32_t *h_in = nullptr, *h_out = nullptr;
   std::vector<long> exps;
+  // GPU-conversion pipeline (uniform-precision calls): two slots, each with
+  // its own stream and staging for one chunk of signals, grown on demand
+  struct ConvSlot {
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    uint32_t *d_in = nullptr, *d_out = nullptr;
+    uint64_t *h_mi = nullptr, *d_mi = nullptr, *h_mo = nullptr, *d_mo = nullptr;
+    int64_t *h_ei = nullptr, *d_ei = nullptr, *h_eo = nullptr, *d_eo = nullptr, *d_es = nullptr;
+    uint8_t *h_si = nullptr, *d_si = nullptr, *h_so = nullptr, *d_so = nullptr;
+  };
+  ConvSlot cv[2];
+  unsigned long cv_chunk = 0;  // signals per chunk the slots hold
+  int cv_nli = 0, cv_nlo = 0;
+  void free_conv() {
+    for (auto &c : cv) {
+      for (void *q : {(void *)c.d_in, (void *)c.d_out, (void *)c.d_mi, (void *)c.d_mo, (void *)c.d_ei,
+                      (void *)c.d_eo, (void *)c.d_es, (void *)c.d_si, (void *)c.d_so})
+        if (q) cudaFree(q);
+      for (void *q : {(void *)c.h_mi, (void *)c.h_mo, (void *)c.h_ei, (void *)c.h_eo, (void *)c.h_si, (void *)c.h_so})
+        if (q) cudaFreeHost(q);
+      if (c.st) cudaStreamDestroy(c.st);
+      if (c.done) cudaEventDestroy(c.done);
+      c = ConvSlot();
+    }
+    cv_chunk = 0;
+  }
   ~mpfft_mp_plan() {
+    free_conv();
     if (d_in) cudaFree(d_in);
     if (d_out) cudaFree(d_out);
     if (h_in) cudaFreeHost(h_in);
@@ -468,10 +496,176 @@ static void mp_fill_nan(mpfr_t *a, unsigned long n) {
   for (unsigned long k = 0; k < n; ++k) mpfr_set_nan(a[k]);
 }
 
+static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int nlo) {
+  if (chunk <= p->cv_chunk && nli <= p->cv_nli && nlo <= p->cv_nlo) return MPFFT_OK;
+  p->free_conv();
+  const size_t comp = (size_t)2 * p->N * chunk;
+  const size_t words = (size_t)2 * p->L * p->N * chunk;
+  bool ok = true;
+  auto dm = [&](void **q, size_t bytes) { ok = ok && cudaMalloc(q, bytes) == cudaSuccess; };
+  auto hm = [&](void **q, size_t bytes) { ok = ok && cudaMallocHost(q, bytes) == cudaSuccess; };
+  for (auto &c : p->cv) {
+    ok = ok && cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) == cudaSuccess;
+    dm((void **)&c.d_in, words * 4);
+    dm((void **)&c.d_out, words * 4);
+    dm((void **)&c.d_mi, comp * nli * 8);
+    hm((void **)&c.h_mi, comp * nli * 8);
+    dm((void **)&c.d_mo, comp * nlo * 8);
+    hm((void **)&c.h_mo, comp * nlo * 8);
+    dm((void **)&c.d_ei, comp * 8);
+    hm((void **)&c.h_ei, comp * 8);
+    dm((void **)&c.d_eo, comp * 8);
+    hm((void **)&c.h_eo, comp * 8);
+    dm((void **)&c.d_si, comp);
+    hm((void **)&c.h_si, comp);
+    dm((void **)&c.d_so, comp);
+    hm((void **)&c.h_so, comp);
+    dm((void **)&c.d_es, chunk * 8);
+  }
+  if (!ok) {
+    cudaGetLastError();
+    p->free_conv();
+    return set_err(MPFFT_ENOMEM, "cannot allocate conversion staging for %lu-signal chunks", chunk);
+  }
+  p->cv_chunk = chunk;
+  p->cv_nli = nli;
+  p->cv_nlo = nlo;
+  return MPFFT_OK;
+}
+
+static inline int nlimbs64(long prec) { return (int)((prec + 63) / 64); }
+
+// All inputs with one limb count and all outputs with one precision: the
+// conversion runs on the GPU and the host only moves raw significand limbs.
+// The batch is processed in chunks through two slots (stream + staging each):
+// while the GPU copies and transforms chunk i, the host scatters chunk i-1's
+// results and gathers chunk i+1's inputs.  Returns -1 when the call does not
+// qualify (mixed precisions).
+static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr, mpfr_t *ini, unsigned long s,
+                              mpfr_t *outr, mpfr_t *outi, unsigned flags) {
+  const unsigned long N = p->N;
+  const long prec_out = mpfr_get_prec(outr[0]);
+  const int nli = nlimbs64(mpfr_get_prec(inr[0])), nlo = nlimbs64(prec_out);
+  std::vector<int> bad(batch, 0);
+  parallel_for((long)batch, 1, [&](long b0, long b1) {
+    for (long b = b0; b < b1; ++b)
+      for (unsigned long q = 0; q < N && !bad[b]; ++q) {
+        mpfr_srcptr a = elem(inr, b, N, q, s), c = elem(ini, b, N, q, s);
+        if (nlimbs64(a->_mpfr_prec) != nli || nlimbs64(c->_mpfr_prec) != nli) bad[b] = 1;
+        else if (outr[b * N + q]->_mpfr_prec != prec_out || outi[b * N + q]->_mpfr_prec != prec_out) bad[b] = 1;
+      }
+  });
+  for (unsigned long b = 0; b < batch; ++b)
+    if (bad[b]) return -1;
+  // chunks of up to 256 signals (a multiple of 32 keeps every warp on one
+  // butterfly), and at most ~256 MiB of staging per slot
+  const size_t per_signal = (size_t)2 * N * ((nli + nlo) * 8 + 2 * 4 * p->L + 18);
+  unsigned long chunk = std::min<unsigned long>(256, std::max<size_t>(32, (256UL << 20) / per_signal));
+  if (chunk >= 32) chunk &= ~31UL;
+  chunk = std::min(chunk, batch);
+  if (int e = mp_conv_reserve(p, chunk, nli, nlo)) return e;
+  const unsigned long nchunks = (batch + chunk - 1) / chunk;
+  const long shift = (flags & MPFFT_SCALED) ? ilog2(N) : 0;
+  const long emin = mpfr_get_emin(), emax = mpfr_get_emax();
+  std::vector<int> nonfin(nchunks, 0);
+
+  auto gather = [&](unsigned long ci) {
+    auto &c = p->cv[ci & 1];
+    const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
+    parallel_for((long)(2 * cb * N), 2048, [&](long x0, long x1) {
+      for (long u = x0; u < x1; ++u) {
+            const long bb = u / (2 * (long)N), part = (u / (long)N) & 1;
+            const unsigned long q = (unsigned long)(u % (long)N);
+            mpfr_srcptr x = elem(part ? ini : inr, b0 + bb, N, q, s);
+            const size_t t = ((size_t)part * N + q) * cb + bb;
+            if (x->_mpfr_exp <= LONG_MIN + 3) {  // MPFR's reserved exponents: zero, NaN, infinity
+              if (!mpfr_zero_p(x)) nonfin[ci] = 1;
+              c.h_ei[t] = INT64_MIN;
+              c.h_si[t] = 0;
+              memset(c.h_mi + t * nli, 0, nli * 8);
+            } else {
+              c.h_ei[t] = x->_mpfr_exp;
+              c.h_si[t] = x->_mpfr_sign < 0;
+              memcpy(c.h_mi + t * nli, x->_mpfr_d, nli * 8);
+            }
+          }
+    });
+  };
+  auto launch = [&](unsigned long ci) -> int {
+    auto &c = p->cv[ci & 1];
+    const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
+    const size_t comp = (size_t)2 * N * cb;
+    CUDA_TRY(cudaMemcpyAsync(c.d_mi, c.h_mi, comp * nli * 8, cudaMemcpyHostToDevice, c.st));
+    CUDA_TRY(cudaMemcpyAsync(c.d_ei, c.h_ei, comp * 8, cudaMemcpyHostToDevice, c.st));
+    CUDA_TRY(cudaMemcpyAsync(c.d_si, c.h_si, comp, cudaMemcpyHostToDevice, c.st));
+    CUDA_TRY(mp_import_launch(c.d_mi, c.d_ei, c.d_si, nli, (int)N, (int)cb, p->L, p->F, c.d_es, c.d_in, c.st));
+    CUDA_TRY(mp_run_transform(p->L, p->tabs, c.d_in, c.d_out, (int)cb, c.st));
+    CUDA_TRY(mp_export_launch(c.d_out, (int)N, (int)cb, p->L, c.d_es, p->F + shift, prec_out, nlo, c.d_mo, c.d_eo,
+                              c.d_so, c.st));
+    CUDA_TRY(cudaMemcpyAsync(c.h_mo, c.d_mo, comp * nlo * 8, cudaMemcpyDeviceToHost, c.st));
+    CUDA_TRY(cudaMemcpyAsync(c.h_eo, c.d_eo, comp * 8, cudaMemcpyDeviceToHost, c.st));
+    CUDA_TRY(cudaMemcpyAsync(c.h_so, c.d_so, comp, cudaMemcpyDeviceToHost, c.st));
+    CUDA_TRY(cudaEventRecord(c.done, c.st));
+    return MPFFT_OK;
+  };
+  auto scatter = [&](unsigned long ci) -> int {
+    auto &c = p->cv[ci & 1];
+    CUDA_TRY(cudaEventSynchronize(c.done));
+    const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
+    parallel_for((long)(2 * cb * N), 2048, [&](long x0, long x1) {
+      for (long u = x0; u < x1; ++u) {
+            const long bb = u / (2 * (long)N), part = (u / (long)N) & 1;
+            const unsigned long q = (unsigned long)(u % (long)N);
+            mpfr_ptr y = (part ? outi : outr)[(b0 + bb) * N + q];
+            const size_t t = ((size_t)part * N + q) * cb + bb;
+            const int64_t e = c.h_eo[t];
+            if (e == INT64_MIN) {
+              mpfr_set_zero(y, 1);
+            } else if (e >= emin && e <= emax) {
+              memcpy(y->_mpfr_d, c.h_mo + t * nlo, nlo * 8);
+              y->_mpfr_exp = e;
+              y->_mpfr_sign = c.h_so[t] ? -1 : 1;
+            } else {  // outside the current exponent range: let MPFR overflow/underflow
+              __mpz_struct z;
+              z._mp_alloc = nlo;
+              z._mp_size = c.h_so[t] ? -nlo : nlo;
+              z._mp_d = reinterpret_cast<mp_limb_t *>(c.h_mo + t * nlo);
+              mpfr_set_z_2exp(y, &z, e - 64L * nlo, MPFR_RNDN);
+            }
+          }
+    });
+    return MPFFT_OK;
+  };
+
+  // validate every input before any output is written
+  int err = MPFFT_OK;
+  gather(0);
+  if (nonfin[0]) return set_err(MPFFT_ENONFINITE, "input holds NaN or infinity");
+  if ((err = launch(0))) return err;
+  for (unsigned long ci = 1; ci < nchunks; ++ci) {
+    if (ci >= 2 && (err = scatter(ci - 2))) return err;  // frees slot ci&1
+    gather(ci);
+    if (nonfin[ci]) {
+      cudaStreamSynchronize(p->cv[0].st);
+      cudaStreamSynchronize(p->cv[1].st);
+      return set_err(MPFFT_ENONFINITE, "input holds NaN or infinity");
+    }
+    if ((err = launch(ci))) return err;
+  }
+  for (unsigned long ci = nchunks >= 2 ? nchunks - 2 : 0; ci < nchunks; ++ci)
+    if ((err = scatter(ci))) return err;
+  return set_err(MPFFT_OK, "");
+}
+
 static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr, mpfr_t *ini, unsigned long s,
                            mpfr_t *outr, mpfr_t *outi, unsigned flags) {
   if (p->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
   std::lock_guard<std::mutex> g(p->mu);
+  if (!p->force_host_conversion) {
+    const int r = mp_execute_gpuconv(p, batch, inr, ini, s, outr, outi, flags);
+    if (r != -1) return r;
+  }
   if (int e = mp_reserve(p, batch)) return e;
   p->exps.assign(batch, 0);
   if (int e = mp_pack_impl(p, batch, inr, ini, s, p->h_in, p->exps.data())) return e;
@@ -684,6 +878,7 @@ MPFFT_API int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, 
   std::unique_ptr<mpfft_mp_plan> p(new (std::nothrow) mpfft_mp_plan);
   if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
   if (int e = mp_plan_init(p.get(), n, prec, (flags & MPFFT_PLAN_HOST_ONLY) != 0)) return e;
+  p->force_host_conversion = (flags & MPFFT_PLAN_HOST_CONVERSION) != 0;
   *plan = p.release();
   return set_err(MPFFT_OK, "");
 }

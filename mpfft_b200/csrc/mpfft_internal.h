@@ -57,6 +57,14 @@ constexpr int kMinLimbs = 2;
 cudaError_t mp_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
                              cudaStream_t s, float *launch_ms = nullptr);
 cudaError_t diag_imad_rate(int wide, double *ops_per_s);
+
+// GPU-side conversion between MPFR significands and limb planes.  Component
+// (c, p, b) is index (c*N + p)*B + b of the mant/ex/sg arrays; ex = INT64_MIN
+// marks zero.  import computes the per-signal block exponents into es[B].
+cudaError_t mp_import_launch(const uint64_t *mant, const int64_t *ex, const uint8_t *sg, int nl, int N, int B,
+                             int L, long F, int64_t *es, uint32_t *planes, cudaStream_t s);
+cudaError_t mp_export_launch(const uint32_t *planes, int N, int B, int L, const int64_t *es, long F_plus_shift,
+                             long prec, int nlo, uint64_t *out, int64_t *oex, uint8_t *osg, cudaStream_t s);
 cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
                             cudaStream_t s);
 

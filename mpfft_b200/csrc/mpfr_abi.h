@@ -60,4 +60,6 @@ int mpfr_rint(mpfr_ptr, mpfr_srcptr, mpfr_rnd_t);
 int mpfr_sgn(mpfr_srcptr);
 int mpfr_sin_cos(mpfr_ptr, mpfr_ptr, mpfr_srcptr, mpfr_rnd_t);
 void mpfr_free_cache(void);
+mpfr_exp_t mpfr_get_emin(void);
+mpfr_exp_t mpfr_get_emax(void);
 }

@@ -198,3 +198,32 @@ def test_mp_large_n_roundtrip(M, orc, n, p):
     assert M.mp_sr24_cp_fft_scaled(n, 1, 0, yi.ptr, yr.ptr, zr.ptr, zi.ptr) == M.OK
     e = O.mp_errors(zi, zr, xr, xi)
     assert e["log2_rel"] <= O.mp_bound_log2(n, p) + 1, e
+
+
+@pytest.mark.parametrize("n,p_in,p_out,batch,scaled", [
+    (1024, 1024, 1024, 64, False), (256, 100, 64, 33, False), (64, 53, 200, 32, True), (16, 64, 64, 3, False),
+    (2, 64, 30, 5, True)])
+def test_mp_gpu_conversion_matches_host_conversion(M, orc, n, p_in, p_out, batch, scaled):
+    """The GPU import/export of significands gives bit-identical outputs to the
+    host conversion (mpfr_set_z_2exp rounding), incl. rounding to a lower output
+    precision, zero signals, negative values and 2^+-40 block scales."""
+    O = orc
+    L = O.lib()
+    prec = max(p_in, p_out)
+    xr, xi = O.mp_pair(n * batch, p_in)
+    O.fill_uniform(xr, xi, 77)
+    for b in range(batch):
+        e = (0, 40, -40, 7, 0)[b % 5]
+        for a in (xr, xi):
+            L.orc_mp_scale2(a.ptr + b * n * 32, n, e)
+    if batch > 1:  # signal 1 entirely zero
+        L.orc_mp_set_ui(xr.ptr + n * 32, n, 0)
+        L.orc_mp_set_ui(xi.ptr + n * 32, n, 0)
+    gpu = M.MpPlan(n, prec)
+    host = M.MpPlan(n, prec, host_conversion=True)
+    yr, yi = O.mp_pair(n * batch, p_out)
+    zr, zi = O.mp_pair(n * batch, p_out)
+    gpu.execute(batch, xr.ptr, xi.ptr, yr.ptr, yi.ptr, scaled=scaled)
+    host.execute(batch, xr.ptr, xi.ptr, zr.ptr, zi.ptr, scaled=scaled)
+    assert L.orc_mp_count_diff(yr.ptr, zr.ptr, n * batch) == 0
+    assert L.orc_mp_count_diff(yi.ptr, zi.ptr, n * batch) == 0
