@@ -712,3 +712,56 @@ OAPI unsigned long long orc_now_ns(void) {
   clock_gettime(CLOCK_MONOTONIC, &t);
   return (unsigned long long)t.tv_sec * 1000000000ULL + (unsigned long long)t.tv_nsec;
 }
+
+/* ------------------------------------------------------------------------ */
+/* raw significand fields (for tests of device-resident significand APIs)   */
+/* ------------------------------------------------------------------------ */
+
+/* Component order (c, p, b) -> index (c*n + p)*batch + b, where re = a_re and
+ * im = a_im hold `batch` signals of n points (signal b at [b*n, (b+1)*n)).
+ * mant: nl 64-bit limbs per component; ex: exponent or INT64_MIN for zero;
+ * sg: 1 for negative.  Returns 0, or -1 if an element is NaN/Inf or has
+ * more than nl limbs. */
+OAPI int orc_mp_export_raw(mpfr_t *a_re, mpfr_t *a_im, unsigned long n, unsigned long batch, int nl,
+                           uint64_t *mant, int64_t *ex, uint8_t *sg) {
+  for (unsigned long b = 0; b < batch; b++)
+    for (int c = 0; c < 2; c++)
+      for (unsigned long p = 0; p < n; p++) {
+        mpfr_ptr x = (c ? a_im : a_re)[b * n + p];
+        size_t t = ((size_t)c * n + p) * batch + b;
+        int xl = (int)((mpfr_get_prec(x) + 63) / 64);
+        if (!mpfr_number_p(x) || xl > nl) return -1;
+        memset(mant + t * nl, 0, (size_t)nl * 8);
+        if (mpfr_zero_p(x)) {
+          ex[t] = INT64_MIN;
+          sg[t] = 0;
+        } else {
+          /* left-align the significand in nl limbs */
+          memcpy(mant + t * nl + (nl - xl), x->_mpfr_d, (size_t)xl * 8);
+          ex[t] = x->_mpfr_exp;
+          sg[t] = x->_mpfr_sign < 0;
+        }
+      }
+  return 0;
+}
+
+/* inverse of orc_mp_export_raw: value = sign * 0.mant * 2^ex, rounded into
+ * each destination element at its own precision */
+OAPI void orc_mp_import_raw(mpfr_t *a_re, mpfr_t *a_im, unsigned long n, unsigned long batch, int nl,
+                            const uint64_t *mant, const int64_t *ex, const uint8_t *sg) {
+  for (unsigned long b = 0; b < batch; b++)
+    for (int c = 0; c < 2; c++)
+      for (unsigned long p = 0; p < n; p++) {
+        mpfr_ptr y = (c ? a_im : a_re)[b * n + p];
+        size_t t = ((size_t)c * n + p) * batch + b;
+        if (ex[t] == INT64_MIN) {
+          mpfr_set_zero(y, 1);
+          continue;
+        }
+        __mpz_struct z;
+        z._mp_alloc = nl;
+        z._mp_size = sg[t] ? -nl : nl;
+        z._mp_d = (mp_limb_t *)(mant + t * nl);
+        mpfr_set_z_2exp(y, &z, (mpfr_exp_t)(ex[t] - 64L * nl), RN);
+      }
+}

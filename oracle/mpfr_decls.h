@@ -20,6 +20,7 @@
 #define MPFFT_MPFR_DECLS_H
 
 #include <stddef.h>
+#include <stdint.h>
 #include <stdio.h>
 
 #ifdef __cplusplus

@@ -76,6 +76,8 @@ def lib() -> C.CDLL:
         "orc_d_fft": (None, [vp, ul, ul, sl, dp, dp, dp, dp]),
         "orc_d_fft_top": (None, [vp, dp, dp, dp, dp]),
         "orc_d_fill_uniform": (None, [dp, dp, ul, ul]),
+        "orc_mp_export_raw": (C.c_int, [vp, vp, ul, ul, C.c_int, vp, vp, vp]),
+        "orc_mp_import_raw": (None, [vp, vp, ul, ul, C.c_int, vp, vp, vp]),
         "orc_mpfr_version": (C.c_char_p, []),
         "orc_now_ns": (C.c_ulonglong, []),
     }
