@@ -147,6 +147,37 @@ int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const double *inr, 
 int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, const double *d_in, double *d_out,
                            unsigned flags, void *stream);
 
+/* Transform `batch` signals whose MPFR fields are already in device memory,
+ * WITHOUT allocating anything: no cudaMalloc, cudaFree or other allocating
+ * call.  No counterpart in the reference.  For callers that cannot allocate
+ * device memory when they call -- services that reserve their whole device
+ * memory budget at start-up, and code paths that must not pay the implicit
+ * device-wide synchronisation of cudaMalloc/cudaFree.  The plan must be
+ * created beforehand (plan creation does allocate).
+ *
+ * Inputs/outputs, component (c, p, b) at index (c*n + p)*batch + b, c = 0 real
+ * / 1 imaginary: significand limbs (nl_in resp. ceil(prec_out/64) 64-bit limbs
+ * per component, least significant first, normalised as in an mpfr_t),
+ * exponents (value = sign * 0.significand * 2^exp; INT64_MIN marks zero) and
+ * signs (1 = negative).  Outputs are rounded to nearest-even at prec_out bits,
+ * as mpfr_set_z_2exp would.  Inputs must be finite.  flags: MPFFT_SCALED.
+ *
+ * Working storage is one static device array of mpfft_static_scratch_bytes()
+ * (64 MiB) that every GPU loading this library holds until the process exits:
+ * a batch needs 16*L*n*batch + 8*batch bytes (L = mpfft_mp_plan_limbs), and
+ * larger batches are rejected with MPFFT_EUNSUPPORTED.  The first call on each
+ * device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current; make that first call before any stream capture.  All calls
+ * share the array and it keeps the last call's contents (every word a call
+ * reads it has written first): calls that overlap on the GPU race, so issue
+ * them on one stream or serialise them.  Asynchronous on `stream`. */
+int mpfft_mp_execute_significands_static(const mpfft_mp_plan *plan, unsigned long batch, const uint64_t *d_mant_in,
+                                         const int64_t *d_exp_in, const uint8_t *d_sign_in, int nl_in,
+                                         uint64_t *d_mant_out, int64_t *d_exp_out, uint8_t *d_sign_out,
+                                         long prec_out, unsigned flags, void *stream);
+/* size in bytes of the static device array used by the entry point above */
+size_t mpfft_static_scratch_bytes(void);
+
 /* ------------------------------------------------------------------------ */
 /* 3. diagnostics for benchmarks (no counterpart in the reference)          */
 /* ------------------------------------------------------------------------ */

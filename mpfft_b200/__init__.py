@@ -73,6 +73,9 @@ def _load() -> C.CDLL:
         "mpfft_mp_plan_schedule": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]),
         "mpfft_mp_execute_device_timed": (C.c_int, [vp, ul, u32p, u32p, vp, C.POINTER(C.c_float)]),
         "mpfft_diag_imad_rate": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+        "mpfft_mp_execute_significands_static": (C.c_int, [vp, ul, vp, vp, vp, C.c_int, vp, vp, vp, sl, C.c_uint,
+                                                           vp]),
+        "mpfft_static_scratch_bytes": (C.c_size_t, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -184,6 +187,13 @@ class MpPlan:
         ms = (C.c_float * (nl + 1))()
         _check(lib.mpfft_mp_execute_device_timed(self.h, batch, d_in, d_out, stream or None, ms))
         return list(ms)
+
+    def execute_significands_static(self, batch, d_mant_in, d_exp_in, d_sign_in, nl_in, d_mant_out, d_exp_out,
+                                    d_sign_out, prec_out, scaled=False, stream: int = 0) -> None:
+        """Device-resident MPFR fields in and out; allocates nothing (static scratch)."""
+        _check(lib.mpfft_mp_execute_significands_static(self.h, batch, d_mant_in, d_exp_in, d_sign_in, nl_in,
+                                                        d_mant_out, d_exp_out, d_sign_out, prec_out,
+                                                        SCALED if scaled else 0, stream or None))
 
     def pack(self, batch, inr, ini, planes_ptr: int, exps_ptr: int) -> None:
         _check(lib.mpfft_mp_pack(self.h, batch, inr, ini, planes_ptr, exps_ptr))

@@ -995,3 +995,33 @@ MPFFT_API int mpfft_diag_imad_rate(int wide, double *ops_per_s) {
   CUDA_TRY(diag_imad_rate(wide, ops_per_s));
   return set_err(MPFFT_OK, "");
 }
+
+// ---------------------------------------------------------------------------
+// entry point without allocation (static scratch, static_scratch.cu)
+// ---------------------------------------------------------------------------
+
+MPFFT_API int mpfft_mp_execute_significands_static(const mpfft_mp_plan *plan, unsigned long batch,
+                                                   const uint64_t *d_mant_in, const int64_t *d_exp_in,
+                                                   const uint8_t *d_sign_in, int nl_in, uint64_t *d_mant_out,
+                                                   int64_t *d_exp_out, uint8_t *d_sign_out, long prec_out,
+                                                   unsigned flags, void *stream) {
+  if (!plan || !d_mant_in || !d_exp_in || !d_sign_in || !d_mant_out || !d_exp_out || !d_sign_out)
+    return set_err(MPFFT_EINVAL, "NULL argument");
+  if (plan->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
+  if (nl_in < 1 || prec_out < 2) return set_err(MPFFT_EINVAL, "nl_in must be >= 1 and prec_out >= 2");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  MpPlanView v;
+  v.N = plan->N;
+  v.L = plan->L;
+  v.F = plan->F;
+  v.tabs = &plan->tabs;
+  char msg[200] = "";
+  const unsigned shift = (flags & MPFFT_SCALED) ? (unsigned)ilog2(plan->N) : 0u;
+  const int rc = mp_execute_significands_static(v, batch, d_mant_in, d_exp_in, d_sign_in, nl_in, d_mant_out,
+                                                d_exp_out, d_sign_out, prec_out, shift, (cudaStream_t)stream, msg,
+                                                sizeof msg);
+  return set_err(rc, "%s", msg);
+}
+
+MPFFT_API size_t mpfft_static_scratch_bytes(void) { return static_scratch_bytes(); }

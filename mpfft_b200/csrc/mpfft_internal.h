@@ -47,6 +47,16 @@ struct DDeviceTables : TreeTables {
   double c8 = 0, c16a = 0, c16b = 0, c16c = 0, c16d = 0;
 };
 
+constexpr int kMaxDevices = 64;
+
+// What the static-scratch entry point needs to know about a plan.
+struct MpPlanView {
+  unsigned long N = 0;
+  int L = 0;
+  long F = 0;
+  const MpDeviceTables *tabs = nullptr;
+};
+
 // largest limb count with register-resident kernels
 constexpr int kMaxLimbs = 34;
 constexpr int kMinLimbs = 2;
@@ -67,5 +77,14 @@ cudaError_t mp_export_launch(const uint32_t *planes, int N, int B, int L, const 
                              long prec, int nlo, uint64_t *out, int64_t *oex, uint8_t *osg, cudaStream_t s);
 cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
                             cudaStream_t s);
+
+// Import -> transform -> export of device-resident MPFR fields with all
+// working storage in a file-scope device array (static_scratch.cu).  Returns an
+// MPFFT_* status and writes a message on failure.
+int mp_execute_significands_static(const MpPlanView &v, unsigned long batch, const uint64_t *d_mant_in,
+                                   const int64_t *d_exp_in, const uint8_t *d_sign_in, int nl_in,
+                                   uint64_t *d_mant_out, int64_t *d_exp_out, uint8_t *d_sign_out, long prec_out,
+                                   unsigned scaled_shift, cudaStream_t stream, char *msg, size_t msglen);
+size_t static_scratch_bytes();
 
 }  // namespace mpfft
