@@ -143,7 +143,8 @@ int mpfft_d_plan_create(mpfft_d_plan **plan, unsigned long n);
 int mpfft_d_plan_destroy(mpfft_d_plan *plan);
 int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const double *inr, const double *ini, double *outr,
                     double *outi, unsigned flags);
-/* Device layout: word (c, p, b) at base[(c*n + p)*batch + b]. */
+/* Device layout: word (c, b, p) at base[(c*batch + b)*n + p], i.e. all real
+ * parts (signal after signal), then all imaginary parts. */
 int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, const double *d_in, double *d_out,
                            unsigned flags, void *stream);
 

@@ -7,10 +7,17 @@
 // association.  This file is compiled with --fmad=false so no multiply-add is
 // contracted into an FMA (the reference's x86-64 build has no FMA either).
 //
-// Schedule: breadth-first over the reference's recursion tree -- one launch
-// for all leaves (n = 16 and 8 for N >= 16; the whole transform for N <= 16),
-// then one launch per node size n = 32 .. N.  Layout: word (c, p, b) at
-// base[(c*N + p)*B + b]; consecutive threads are consecutive signals (or k).
+// Schedule: the reference's recursion tree, cut at T = min(N, 4096) points.
+// Every maximal node of size <= T (size T or T/2) is one shared-memory
+// sub-transform: one CTA gathers its input sequence in DIT order (so every
+// leaf's inputs already sit where its outputs go), runs the leaves (n = 16 and
+// 8; the whole transform for N <= 16) and all levels up to the node in place
+// in shared memory, and writes the node's outputs once.  Levels above T run
+// one launch per node size in global memory.  For N <= 4096 a transform is one
+// launch that reads its input once and writes its output once.
+//
+// Layout: word (c, b, p) at base[(c*B + b)*N + p] -- each signal contiguous.
+#include <algorithm>
 #include <cstdint>
 
 #include "mpfft_internal.h"
@@ -93,85 +100,227 @@ __device__ __forceinline__ void d16_part(const DConst &K, const double *x, bool 
   o.c20 = c14 - c16;
 }
 
-__global__ void __launch_bounds__(128) d_leaf_kernel(const double *__restrict__ in, double *__restrict__ out, int N,
-                                                      int B, const Leaf *__restrict__ leaves, int nleaves, DConst K,
-                                                      double scale) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)nleaves * B) return;
-  const int b = (int)(t % B);
-  const Leaf lf = leaves[t / B];
-  const size_t cim = (size_t)N * B;
-  double xr[16], xi[16], yr[16], yi[16];
-  const int n = lf.n;
+// Shared-memory index with one pad slot per 16 elements: leaves work on 16
+// (or 8) consecutive elements per thread, so without padding every lane of a
+// warp would hit the same banks.
+__device__ __forceinline__ int pidx(int m) { return m + (m >> 4); }
+
+// Leaf of size 16 at positions [o, o+16) (reference :213-385), in place.
+__device__ __forceinline__ void d_leaf16(const DConst &K, double *yr, double *yi, int o) {
+  double xr[16], xi[16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    if (j < n) {
-      const int idx = (j == 0 && lf.sn < 0) ? lf.sn + N : lf.sn + j * lf.s;
-      xr[j] = in[(size_t)idx * B + b];
-      xi[j] = in[(size_t)idx * B + b + cim];
-    } else {
-      xr[j] = 0.0;
-      xi[j] = 0.0;
-    }
+    xr[j] = yr[pidx(o + j)];
+    xi[j] = yi[pidx(o + j)];
   }
-  if (n == 16) {
-    D16 R, I;
-    d16_part(K, xr, false, R);
-    d16_part(K, xi, true, I);
-    // output stage (reference :350-382)
-    yr[0] = R.b5 + R.b11;  yr[8] = R.b5 - R.b11;
-    yi[0] = I.b5 + I.b11;  yi[8] = I.b5 - I.b11;
-    yr[4] = R.b6 - I.b12;  yr[12] = R.b6 + I.b12;
-    yi[4] = I.b6 - R.b12;  yi[12] = I.b6 + R.b12;
-    yr[1] = R.c9 - I.c17;  yr[15] = R.c9 + I.c17;
-    yi[1] = I.c9 - R.c17;  yi[15] = I.c9 + R.c17;
-    yr[2] = R.c1 - I.c3;   yr[14] = R.c1 + I.c3;
-    yi[2] = I.c1 - R.c3;   yi[14] = I.c1 + R.c3;
-    yr[3] = R.c12 + I.c20; yr[13] = R.c12 - I.c20;
-    yi[3] = I.c12 + R.c20; yi[13] = I.c12 - R.c20;
-    yr[5] = R.c11 - I.c19; yr[11] = R.c11 + I.c19;
-    yi[5] = I.c11 - R.c19; yi[11] = I.c11 + R.c19;
-    yr[6] = R.c2 - I.c4;   yr[10] = R.c2 + I.c4;
-    yi[6] = I.c2 - R.c4;   yi[10] = I.c2 + R.c4;
-    yr[7] = R.c10 + I.c18; yr[9] = R.c10 - I.c18;
-    yi[7] = I.c10 + R.c18; yi[9] = I.c10 - R.c18;
-  } else if (n == 8) {
-    double R[8], I[8];
-    d8_part(K, xr, R);
-    d8_part(K, xi, I);
-    // output stage (reference :193-209)
-    yr[0] = R[1] + R[0]; yr[4] = R[1] - R[0];
-    yi[0] = I[1] + I[0]; yi[4] = I[1] - I[0];
-    yr[1] = R[4] + I[6]; yr[7] = R[4] - I[6];
-    yi[1] = I[4] - R[6]; yi[7] = I[4] + R[6];
-    yr[2] = R[2] + I[3]; yr[6] = R[2] - I[3];
-    yi[2] = I[2] - R[3]; yi[6] = I[2] + R[3];
-    yr[3] = R[5] - I[7]; yr[5] = R[5] + I[7];
-    yi[3] = I[5] + R[7]; yi[5] = I[5] - R[7];
-  } else if (n == 4) {
-    // reference :121-147
+  D16 R, I;
+  d16_part(K, xr, false, R);
+  d16_part(K, xi, true, I);
+  // output stage (reference :350-382)
+  double *r = yr, *i = yi;
+#define P(j) pidx(o + (j))
+  r[P(0)] = R.b5 + R.b11;  r[P(8)] = R.b5 - R.b11;
+  i[P(0)] = I.b5 + I.b11;  i[P(8)] = I.b5 - I.b11;
+  r[P(4)] = R.b6 - I.b12;  r[P(12)] = R.b6 + I.b12;
+  i[P(4)] = I.b6 - R.b12;  i[P(12)] = I.b6 + R.b12;
+  r[P(1)] = R.c9 - I.c17;  r[P(15)] = R.c9 + I.c17;
+  i[P(1)] = I.c9 - R.c17;  i[P(15)] = I.c9 + R.c17;
+  r[P(2)] = R.c1 - I.c3;   r[P(14)] = R.c1 + I.c3;
+  i[P(2)] = I.c1 - R.c3;   i[P(14)] = I.c1 + R.c3;
+  r[P(3)] = R.c12 + I.c20; r[P(13)] = R.c12 - I.c20;
+  i[P(3)] = I.c12 + R.c20; i[P(13)] = I.c12 - R.c20;
+  r[P(5)] = R.c11 - I.c19; r[P(11)] = R.c11 + I.c19;
+  i[P(5)] = I.c11 - R.c19; i[P(11)] = I.c11 + R.c19;
+  r[P(6)] = R.c2 - I.c4;   r[P(10)] = R.c2 + I.c4;
+  i[P(6)] = I.c2 - R.c4;   i[P(10)] = I.c2 + R.c4;
+  r[P(7)] = R.c10 + I.c18; r[P(9)] = R.c10 - I.c18;
+  i[P(7)] = I.c10 + R.c18; i[P(9)] = I.c10 - R.c18;
+#undef P
+}
+
+// Leaf of size 8 at positions [o, o+8) (reference :148-212), in place.
+__device__ __forceinline__ void d_leaf8(const DConst &K, double *yr, double *yi, int o) {
+  double xr[8], xi[8], R[8], I[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    xr[j] = yr[pidx(o + j)];
+    xi[j] = yi[pidx(o + j)];
+  }
+  d8_part(K, xr, R);
+  d8_part(K, xi, I);
+  // output stage (reference :193-209)
+#define P(j) pidx(o + (j))
+  yr[P(0)] = R[1] + R[0]; yr[P(4)] = R[1] - R[0];
+  yi[P(0)] = I[1] + I[0]; yi[P(4)] = I[1] - I[0];
+  yr[P(1)] = R[4] + I[6]; yr[P(7)] = R[4] - I[6];
+  yi[P(1)] = I[4] - R[6]; yi[P(7)] = I[4] + R[6];
+  yr[P(2)] = R[2] + I[3]; yr[P(6)] = R[2] - I[3];
+  yi[P(2)] = I[2] - R[3]; yi[P(6)] = I[2] + R[3];
+  yr[P(3)] = R[5] - I[7]; yr[P(5)] = R[5] + I[7];
+  yi[P(3)] = I[5] + R[7]; yi[P(5)] = I[5] - R[7];
+#undef P
+}
+
+// Leaves of size 4, 2, 1 (only when the whole transform has N <= 4).
+__device__ __forceinline__ void d_leaf_small(double *yr, double *yi, int o, int n) {
+  double xr[4], xi[4];
+  for (int j = 0; j < n; ++j) {
+    xr[j] = yr[pidx(o + j)];
+    xi[j] = yi[pidx(o + j)];
+  }
+  if (n == 4) {  // reference :121-147
     const double er = xr[0] + xr[2], fr = xr[0] - xr[2], gr = xr[1] + xr[3], hr = xr[1] - xr[3];
     const double ei = xi[0] + xi[2], fi = xi[0] - xi[2], gi = xi[1] + xi[3], hi = xi[1] - xi[3];
-    yr[0] = er + gr; yr[1] = fr + hi; yr[2] = er - gr; yr[3] = fr - hi;
-    yi[0] = ei + gi; yi[1] = fi - hr; yi[2] = ei - gi; yi[3] = fi + hr;
-  } else if (n == 2) {
-    yr[0] = xr[0] + xr[1]; yr[1] = xr[0] - xr[1];
-    yi[0] = xi[0] + xi[1]; yi[1] = xi[0] - xi[1];
-  } else {
-    yr[0] = xr[0];
-    yi[0] = xi[0];
-  }
-  double *y = out + (size_t)lf.out * B + b;
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    if (j < n) {
-      y[(size_t)j * B] = yr[j] * scale;
-      y[(size_t)j * B + cim] = yi[j] * scale;
-    }
+    yr[pidx(o + 0)] = er + gr; yr[pidx(o + 1)] = fr + hi; yr[pidx(o + 2)] = er - gr; yr[pidx(o + 3)] = fr - hi;
+    yi[pidx(o + 0)] = ei + gi; yi[pidx(o + 1)] = fi - hr; yi[pidx(o + 2)] = ei - gi; yi[pidx(o + 3)] = fi + hr;
+  } else if (n == 2) {  // reference :108-120
+    yr[pidx(o)] = xr[0] + xr[1]; yr[pidx(o + 1)] = xr[0] - xr[1];
+    yi[pidx(o)] = xi[0] + xi[1]; yi[pidx(o + 1)] = xi[0] - xi[1];
   }
 }
 
-// 4m2a butterflies of all nodes of size n (reference :392-427)
+// 4m2a butterfly k of a node of size n at y[off..) (reference :392-427)
+__device__ __forceinline__ void d_butterfly(double *yr, double *yi, size_t stride, int off, int k, int q,
+                                            double w_r, double w_i, double scale) {
+  double *r0 = yr + (size_t)(off + k) * stride, *i0 = yi + (size_t)(off + k) * stride;
+  const size_t qs = (size_t)q * stride;
+  const double u0r = r0[0], u1r = r0[qs], zpr = r0[2 * qs], zmr = r0[3 * qs];
+  const double u0i = i0[0], u1i = i0[qs], zpi = i0[2 * qs], zmi = i0[3 * qs];
+  const double pr = w_r * zpr + w_i * zpi, pi = w_r * zpi - w_i * zpr;
+  const double mr = w_r * zmr - w_i * zmi, mi = w_r * zmi + w_i * zmr;
+  const double sr = pr + mr, si = pi + mi, dr = pr - mr, di = pi - mi;
+  r0[0] = (u0r + sr) * scale;
+  r0[2 * qs] = (u0r - sr) * scale;
+  r0[qs] = (u1r + di) * scale;
+  r0[3 * qs] = (u1r - di) * scale;
+  i0[0] = (u0i + si) * scale;
+  i0[2 * qs] = (u0i - si) * scale;
+  i0[qs] = (u1i - dr) * scale;
+  i0[3 * qs] = (u1i + dr) * scale;
+}
+
+// 4m2a butterfly in shared memory (padded indices)
+__device__ __forceinline__ void d_butterfly_smem(double *yr, double *yi, int off, int k, int q, double w_r,
+                                                 double w_i, double scale) {
+  const int a0 = pidx(off + k), a1 = pidx(off + k + q), a2 = pidx(off + k + 2 * q), a3 = pidx(off + k + 3 * q);
+  const double u0r = yr[a0], u1r = yr[a1], zpr = yr[a2], zmr = yr[a3];
+  const double u0i = yi[a0], u1i = yi[a1], zpi = yi[a2], zmi = yi[a3];
+  const double pr = w_r * zpr + w_i * zpi, pi = w_r * zpi - w_i * zpr;
+  const double mr = w_r * zmr - w_i * zmi, mi = w_r * zmi + w_i * zmr;
+  const double sr = pr + mr, si = pi + mi, dr = pr - mr, di = pi - mi;
+  yr[a0] = (u0r + sr) * scale;
+  yr[a2] = (u0r - sr) * scale;
+  yr[a1] = (u1r + di) * scale;
+  yr[a3] = (u1r - di) * scale;
+  yi[a0] = (u0i + si) * scale;
+  yi[a2] = (u0i - si) * scale;
+  yi[a1] = (u1i - dr) * scale;
+  yi[a3] = (u1i + dr) * scale;
+}
+
+// One CTA = G instances (sub-transform root x signal) entirely in shared
+// memory.  SINGLE: N < 4096, one root per signal, G signals per CTA, all with
+// the big schedule.  Otherwise G = 1 and the CTA's root may be of size T or
+// T/2.  Per instance: gather the root's input sequence in input order
+// (coalesced reads) into DIT positions, leaves, levels, then write the outputs
+// once.  The twiddles the levels need, LUT[m*(N/T)] for m < T/4, are staged in
+// shared memory once per CTA.
+template <bool SINGLE>
+__global__ void __launch_bounds__(256, 2) d_sub_kernel(const double *__restrict__ in, double *__restrict__ out, int N,
+                                                        int B, const SubRoot *__restrict__ roots, int nroots, int G,
+                                                        SubSchedule big, SubSchedule small,
+                                                        const double *__restrict__ wr, const double *__restrict__ wi,
+                                                        DConst K, double scale) {
+  extern __shared__ double sm[];
+  const int Tmax = big.size;
+  const int lgT = 31 - __clz(Tmax);
+  const int istride = 2 * (pidx(Tmax) + 1);  // doubles per instance
+  double *twr = sm + (size_t)G * istride, *twi = twr + Tmax / 4 + 1;
+  for (int m = threadIdx.x; m < Tmax / 4; m += blockDim.x) {
+    twr[m] = wr[(size_t)m * (N / Tmax)];
+    twi[m] = wi[(size_t)m * (N / Tmax)];
+  }
+  // this CTA's instances
+  int G_here, b0;
+  SubRoot rt;
+  bool is_big = true;
+  if (SINGLE) {
+    b0 = blockIdx.x * G;
+    G_here = min(G, B - b0);
+    rt = roots[0];
+  } else {
+    const int root = blockIdx.x % nroots;
+    b0 = blockIdx.x / nroots;
+    G_here = 1;
+    rt = roots[root];
+    is_big = rt.size == Tmax;
+  }
+  const int T = rt.size;
+  const int *perm = is_big ? big.perm : small.perm;
+  const Leaf *leaves = is_big ? big.leaves : small.leaves;
+  const int nleaves = is_big ? big.nleaves : small.nleaves;
+  const int n16 = is_big ? big.nleaf16 : small.nleaf16, n8 = is_big ? big.nleaf8 : small.nleaf8;
+  const int nlevels = is_big ? big.nlevels : small.nlevels;
+  // gather: element j of instance g to DIT position perm[j]
+  for (int e = threadIdx.x; e < (G_here << lgT); e += blockDim.x) {
+    const int g = e >> lgT, j = e & (Tmax - 1);
+    if (!SINGLE && j >= T) continue;
+    int idx = rt.sn + j * rt.s;
+    if (idx < 0) idx += N;
+    const int b = b0 + g;
+    double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
+    const int m = perm[j];
+    yr[pidx(m)] = in[(size_t)b * N + idx];
+    yi[pidx(m)] = in[((size_t)B + b) * N + idx];
+  }
+  __syncthreads();
+  // leaves, grouped by size: 16-point, then 8-point, then (N <= 4 only) smaller
+  for (int e = threadIdx.x; e < G_here * nleaves; e += blockDim.x) {
+    const int g = SINGLE ? e / nleaves : 0, l = SINGLE ? e - g * nleaves : e;
+    double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
+    const Leaf lf = leaves[l];
+    if (l < n16) d_leaf16(K, yr, yi, lf.out);
+    else if (l < n16 + n8) d_leaf8(K, yr, yi, lf.out);
+    else d_leaf_small(yr, yi, lf.out, lf.n);
+  }
+  if (nlevels == 0 && scale != 1.0) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < (G_here << lgT); e += blockDim.x) {
+      const int g = e >> lgT, m = e & (Tmax - 1);
+      double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
+      yr[pidx(m)] *= scale;
+      yi[pidx(m)] *= scale;
+    }
+  }
+  // levels (the small schedule's levels are the big one's minus the last)
+  for (int lv = 0; lv < nlevels; ++lv) {
+    __syncthreads();
+    const int n = big.level_n[lv], q = n >> 2, lgq = 29 - __clz(n);
+    const int cnt = is_big ? big.level_count[lv] : small.level_count[lv];
+    const int *nodes = (is_big ? big.node_off : small.node_off) + (is_big ? big.level_start[lv] : small.level_start[lv]);
+    const int per = cnt * q;
+    const double sc = lv == nlevels - 1 ? scale : 1.0;
+    for (int e = threadIdx.x; e < G_here * per; e += blockDim.x) {
+      const int g = SINGLE ? e / per : 0, t = SINGLE ? e - g * per : e;
+      const int node = t >> lgq, k = t & (q - 1);
+      const int km = k << (lgT - (lgq + 2));  // k * (T/n)
+      double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
+      d_butterfly_smem(yr, yi, nodes[node], k, q, twr[km], twi[km], sc);
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < (G_here << lgT); e += blockDim.x) {
+    const int g = e >> lgT, m = e & (Tmax - 1);
+    if (!SINGLE && m >= T) continue;
+    const int b = b0 + g;
+    const double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
+    out[(size_t)b * N + rt.out + m] = yr[pidx(m)];
+    out[((size_t)B + b) * N + rt.out + m] = yi[pidx(m)];
+  }
+}
+
+// 4m2a butterflies of all nodes of size n above the shared-memory
+// sub-transforms; consecutive threads are consecutive k of one signal.
 __global__ void __launch_bounds__(256) d_level_kernel(double *__restrict__ y, int N, int B, int n,
                                                        const int *__restrict__ node_off, int nnodes,
                                                        const double *__restrict__ wr, const double *__restrict__ wi,
@@ -179,47 +328,50 @@ __global__ void __launch_bounds__(256) d_level_kernel(double *__restrict__ y, in
   const int q = n >> 2;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)nnodes * q * B) return;
-  const int b = (int)(t % B);
-  const long long r = t / B;
-  const int k = (int)(r % q);
-  const int off = node_off[r / q];
-  const size_t cim = (size_t)N * B;
-  double *p0 = y + (size_t)(off + k) * B + b;
-  double *p1 = p0 + (size_t)q * B, *p2 = p0 + (size_t)2 * q * B, *p3 = p0 + (size_t)3 * q * B;
+  const int k = (int)(t % q);
+  const long long r = t / q;
+  const int node = (int)(r % nnodes);
+  const int b = (int)(r / nnodes);
   const int kn = k * (N / n);
-  const double w_r = wr[kn], w_i = wi[kn];
-  const double u0r = p0[0], u1r = p1[0], zpr = p2[0], zmr = p3[0];
-  const double u0i = p0[cim], u1i = p1[cim], zpi = p2[cim], zmi = p3[cim];
-  const double pr = w_r * zpr + w_i * zpi, pi = w_r * zpi - w_i * zpr;
-  const double mr = w_r * zmr - w_i * zmi, mi = w_r * zmi + w_i * zmr;
-  const double sr = pr + mr, si = pi + mi, dr = pr - mr, di = pi - mi;
-  p0[0] = (u0r + sr) * scale;
-  p2[0] = (u0r - sr) * scale;
-  p1[0] = (u1r + di) * scale;
-  p3[0] = (u1r - di) * scale;
-  p0[cim] = (u0i + si) * scale;
-  p2[cim] = (u0i - si) * scale;
-  p1[cim] = (u1i - dr) * scale;
-  p3[cim] = (u1i + dr) * scale;
+  d_butterfly(y + (size_t)b * N, y + ((size_t)B + b) * N, 1, node_off[node], k, q, wr[kn], wi[kn], scale);
+}
+
+// instances of the shared-memory kernel per CTA and its dynamic shared memory
+static int d_sub_instances(const DDeviceTables &T) {
+  if (T.nroots != 1) return 1;
+  const int per = 2 * (T.sub[0].size + T.sub[0].size / 16 + 1);
+  return std::max(1, std::min(kDSubMax / std::max(T.sub[0].size, 1), 8192 / per));
 }
 
 cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
                             cudaStream_t s) {
   const DConst K{T.c8, T.c16a, T.c16b, T.c16c, T.c16d};
-  {
-    const int threads = 128;
-    const long long total = (long long)T.nleaves * B;
-    const int blocks = (int)((total + threads - 1) / threads);
-    d_leaf_kernel<<<blocks, threads, 0, s>>>(in, out, T.N, B, T.leaves, T.nleaves, K,
-                                             T.nlevels == 0 ? scale : 1.0);
+  const int size = T.sub[0].size;
+  const int G = d_sub_instances(T);
+  const size_t smem = ((size_t)G * 2 * (size + size / 16 + 1) + 2 * (size / 4 + 1)) * sizeof(double);
+  static bool attr_set = false;  // idempotent; benign race
+  if (!attr_set) {
+    cudaFuncSetAttribute(d_sub_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+    cudaFuncSetAttribute(d_sub_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+    attr_set = true;
   }
-  for (int lv = 0; lv < T.nlevels; ++lv) {
+  const bool final_sub = T.upper.nlevels == 0;
+  if (T.nroots == 1) {
+    const int blocks = (B + G - 1) / G;
+    d_sub_kernel<true><<<blocks, 256, smem, s>>>(in, out, T.N, B, T.roots, T.nroots, G, T.sub[0], T.sub[1], T.wr,
+                                                 T.wi, K, final_sub ? scale : 1.0);
+  } else {
+    d_sub_kernel<false><<<T.nroots * B, 256, smem, s>>>(in, out, T.N, B, T.roots, T.nroots, 1, T.sub[0], T.sub[1],
+                                                        T.wr, T.wi, K, final_sub ? scale : 1.0);
+  }
+  for (int lv = 0; lv < T.upper.nlevels; ++lv) {
     const int threads = 256;
-    const int n = T.level_n[lv];
-    const long long total = (long long)T.level_count[lv] * (n / 4) * B;
-    const int blocks = (int)((total + threads - 1) / threads);
-    d_level_kernel<<<blocks, threads, 0, s>>>(out, T.N, B, n, T.node_off + T.level_start[lv], T.level_count[lv],
-                                              T.wr, T.wi, lv == T.nlevels - 1 ? scale : 1.0);
+    const int n = T.upper.level_n[lv];
+    const long long total = (long long)T.upper.level_count[lv] * (n / 4) * B;
+    const int lblocks = (int)((total + threads - 1) / threads);
+    d_level_kernel<<<lblocks, threads, 0, s>>>(out, T.N, B, n, T.upper.node_off + T.upper.level_start[lv],
+                                               T.upper.level_count[lv], T.wr, T.wi,
+                                               lv == T.upper.nlevels - 1 ? scale : 1.0);
   }
   return cudaGetLastError();
 }

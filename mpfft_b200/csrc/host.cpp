@@ -335,7 +335,8 @@ struct mpfft_mp_plan {
 
 struct mpfft_d_plan {
   unsigned long N = 0;
-  DeviceTree tree;
+  DeviceTree upper;                   // levels above the shared-memory sub-transforms
+  std::vector<void *> dev_allocs;     // roots, perms, sub-schedule tables
   double *d_wr = nullptr, *d_wi = nullptr;
   DDeviceTables tabs;
   cudaStream_t stream = nullptr;
@@ -343,6 +344,7 @@ struct mpfft_d_plan {
   size_t cap = 0;
   double *d_in = nullptr, *d_out = nullptr, *h_in = nullptr, *h_out = nullptr;
   ~mpfft_d_plan() {
+    for (void *q : dev_allocs) cudaFree(q);
     if (d_wr) cudaFree(d_wr);
     if (d_wi) cudaFree(d_wi);
     if (d_in) cudaFree(d_in);
@@ -711,13 +713,71 @@ static void mp_dropin(unsigned long n, unsigned long s, long sn, mpfr_t *inr, mp
 // ---------------------------------------------------------------------------
 // FP64 plans
 // ---------------------------------------------------------------------------
+template <typename T>
+static int upload(mpfft_d_plan *p, const std::vector<T> &v, const T **out) {
+  T *d = nullptr;
+  const size_t bytes = std::max<size_t>(1, v.size()) * sizeof(T);
+  CUDA_TRY(cudaMalloc(&d, bytes));
+  p->dev_allocs.push_back(d);
+  if (!v.empty()) CUDA_TRY(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *out = d;
+  return MPFFT_OK;
+}
+
+// Schedule of a shared-memory sub-transform of `size` points: the leaves and
+// levels of its own recursion tree, and the DIT input order perm[m].
+static int build_sub(mpfft_d_plan *p, int size, SubSchedule &S) {
+  HostTree t;
+  walk(t, size, 1, 0, 0, 16);
+  // invperm[j] = DIT position of element j of the sub-transform's input sequence
+  std::vector<int> perm(size);
+  for (const Leaf &lf : t.leaves)
+    for (int j = 0; j < lf.n; ++j) perm[(j == 0 && lf.sn < 0) ? lf.sn + size : lf.sn + j * lf.s] = lf.out + j;
+  std::vector<int> nodes;
+  std::stable_sort(t.leaves.begin(), t.leaves.end(), [](const Leaf &a, const Leaf &b) { return a.n > b.n; });
+  S.size = size;
+  S.nleaves = (int)t.leaves.size();
+  S.nleaf16 = (int)std::count_if(t.leaves.begin(), t.leaves.end(), [](const Leaf &l) { return l.n == 16; });
+  S.nleaf8 = (int)std::count_if(t.leaves.begin(), t.leaves.end(), [](const Leaf &l) { return l.n == 8; });
+  S.nlevels = 0;
+  for (auto &kv : t.levels) {
+    if (S.nlevels >= kMaxLevels) return set_err(MPFFT_EUNSUPPORTED, "sub-transform too large");
+    S.level_n[S.nlevels] = kv.first;
+    S.level_start[S.nlevels] = (int)nodes.size();
+    S.level_count[S.nlevels] = (int)kv.second.size();
+    nodes.insert(nodes.end(), kv.second.begin(), kv.second.end());
+    ++S.nlevels;
+  }
+  if (int e = upload(p, perm, &S.perm)) return e;
+  if (int e = upload(p, t.leaves, &S.leaves)) return e;
+  if (int e = upload(p, nodes, &S.node_off)) return e;
+  return MPFFT_OK;
+}
+
 static int d_plan_init(mpfft_d_plan *p, unsigned long n) {
   if (!is_pow2(n)) return set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
   if (n > (1UL << 28)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
   if (int e = device_ready()) return e;
   p->N = n;
-  if (int e = build_tree(p->tree, n, 16)) return e;
-  static_cast<TreeTables &>(p->tabs) = p->tree.tabs;
+  p->tabs.N = (int)n;
+  // cut the tree at T points: maximal nodes of size <= T run in shared memory
+  const int T = (int)std::min<unsigned long>(n, kDSubMax);
+  {
+    HostTree t;
+    walk(t, (int)n, 1, 0, 0, T);
+    std::vector<SubRoot> roots;
+    for (const Leaf &lf : t.leaves) roots.push_back(SubRoot{lf.sn, lf.s, lf.out, lf.n});
+    p->tabs.nroots = (int)roots.size();
+    if (int e = upload(p, roots, &p->tabs.roots)) return e;
+    if (int e = build_tree(p->upper, n, T)) return e;  // its levels are the ones above T
+    p->tabs.upper = p->upper.tabs;
+  }
+  if (int e = build_sub(p, T, p->tabs.sub[0])) return e;
+  if (T >= 2) {
+    if (int e = build_sub(p, T / 2, p->tabs.sub[1])) return e;
+  } else {
+    p->tabs.sub[1] = p->tabs.sub[0];
+  }
   // twiddles exactly as the reference lut() (serial_d_fft6.c:52-62)
   const unsigned long q = n / 4;
   std::vector<double> wr(q ? q : 1), wi(q ? q : 1);
@@ -779,22 +839,23 @@ static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *in
   if (int e = d_reserve(p, batch)) return e;
   const unsigned long N = p->N;
   const size_t cim = (size_t)N * batch;
-  // [c][p][b] planes
-  for (unsigned long b = 0; b < batch; ++b)
-    for (unsigned long k = 0; k < N; ++k) {
-      p->h_in[k * batch + b] = inr[(b * N + k) * s];
-      p->h_in[cim + k * batch + b] = ini[(b * N + k) * s];
+  // [c][b][p]: each signal contiguous
+  if (s == 1) {
+    memcpy(p->h_in, inr, cim * sizeof(double));
+    memcpy(p->h_in + cim, ini, cim * sizeof(double));
+  } else {
+    for (size_t t = 0; t < cim; ++t) {
+      p->h_in[t] = inr[t * s];
+      p->h_in[cim + t] = ini[t * s];
     }
+  }
   const size_t bytes = 2 * cim * sizeof(double);
   CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, bytes, cudaMemcpyHostToDevice, p->stream));
   CUDA_TRY(d_run_transform(p->tabs, p->d_in, p->d_out, (int)batch, d_scale(p, flags), p->stream));
   CUDA_TRY(cudaMemcpyAsync(p->h_out, p->d_out, bytes, cudaMemcpyDeviceToHost, p->stream));
   CUDA_TRY(cudaStreamSynchronize(p->stream));
-  for (unsigned long b = 0; b < batch; ++b)
-    for (unsigned long k = 0; k < N; ++k) {
-      outr[b * N + k] = p->h_out[k * batch + b];
-      outi[b * N + k] = p->h_out[cim + k * batch + b];
-    }
+  memcpy(outr, p->h_out, cim * sizeof(double));
+  memcpy(outi, p->h_out + cim, cim * sizeof(double));
   return set_err(MPFFT_OK, "");
 }
 

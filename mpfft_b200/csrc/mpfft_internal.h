@@ -41,13 +41,44 @@ struct MpDeviceTables : TreeTables {
   const uint8_t *dneg = nullptr;  // [N/4]: sign of cos-sin
 };
 
-struct DDeviceTables : TreeTables {
+// Schedule of one shared-memory sub-transform of size `size` (FP64 tier):
+// perm[j] = the position that element j of the sub-transform's input sequence
+// takes (the DIT input order), then the leaves (n <= 16, in place over
+// positions [out, out+n)) and the levels of the size-`size` tree.
+struct SubSchedule {
+  int size = 0;
+  const int *perm = nullptr;
+  int nleaves = 0;
+  int nleaf16 = 0, nleaf8 = 0;   // leaves are sorted: 16-point, 8-point, then smaller
+  const Leaf *leaves = nullptr;  // .sn/.s unused: inputs are already in place
+  int nlevels = 0;
+  int level_n[kMaxLevels] = {};
+  int level_start[kMaxLevels] = {};
+  int level_count[kMaxLevels] = {};
+  const int *node_off = nullptr;
+};
+
+// root of a shared-memory sub-transform: input elements x[(sn + j*s)] (j = 0
+// wrapped to sn + N when sn < 0), outputs y[out .. out+size)
+struct SubRoot {
+  int sn, s, out, size;
+};
+
+struct DDeviceTables {
+  int N = 0;
   const double *wr = nullptr;  // [N/4] cos(2 pi k/N)
   const double *wi = nullptr;  // [N/4] sin(2 pi k/N)
   double c8 = 0, c16a = 0, c16b = 0, c16c = 0, c16d = 0;
+  // shared-memory sub-transforms (sizes T and T/2) ...
+  int nroots = 0;
+  const SubRoot *roots = nullptr;
+  SubSchedule sub[2];
+  // ... and the levels above them, in global memory
+  TreeTables upper;
 };
 
 constexpr int kMaxDevices = 64;
+constexpr int kDSubMax = 4096;  // FP64: largest shared-memory sub-transform (64 KB)
 
 // What the static-scratch entry point needs to know about a plan.
 struct MpPlanView {
@@ -75,6 +106,7 @@ cudaError_t mp_import_launch(const uint64_t *mant, const int64_t *ex, const uint
                              int L, long F, int64_t *es, uint32_t *planes, cudaStream_t s);
 cudaError_t mp_export_launch(const uint32_t *planes, int N, int B, int L, const int64_t *es, long F_plus_shift,
                              long prec, int nlo, uint64_t *out, int64_t *oex, uint8_t *osg, cudaStream_t s);
+// FP64 layout: word (c, b, p) at base[(c*B + b)*N + p]  (signal-contiguous)
 cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
                             cudaStream_t s);
 

@@ -30,17 +30,47 @@ def synthetic_planes(n: int, limbs: int, frac_bits: int, batch: int, seed: int =
     return words.reshape(-1)
 
 
+def run_fp64(a) -> None:
+    """FP64 tier: batch of signals in the device layout [c][b][p]; reports
+    time per transform batch and in+out bytes / time."""
+    import torch
+
+    import mpfft_b200 as M
+
+    plan = M.DPlan(a.n)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    d_in = torch.rand((2, a.batch, a.n), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    d_out = torch.empty_like(d_in)
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        plan.execute_device(a.batch, d_in.data_ptr(), d_out.data_ptr(), stream=s.cuda_stream)
+    e0.record(s)
+    for _ in range(a.reps):
+        plan.execute_device(a.batch, d_in.data_ptr(), d_out.data_ptr(), stream=s.cuda_stream)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.reps
+    nbytes = 2 * d_in.numel() * 8
+    print(f"fp64 n={a.n} batch={a.batch}: {ms:.4f} ms per batch, {a.batch / ms * 1e3:.0f} FFT/s, "
+          f"in+out {nbytes / ms / 1e6:.0f} GB/s")
+
+
 def main():
     import torch
 
     import mpfft_b200 as M
 
     ap = argparse.ArgumentParser()
+    ap.add_argument("--tier", default="mp", choices=["mp", "fp64"])
     ap.add_argument("--n", type=int, default=1024)
     ap.add_argument("--prec", type=int, default=1024)
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--reps", type=int, default=2)
     a = ap.parse_args()
+    if a.tier == "fp64":
+        run_fp64(a)
+        return
     plan = M.MpPlan(a.n, a.prec)
     host = synthetic_planes(a.n, plan.limbs, plan.frac_bits, a.batch)
     d_in = torch.from_numpy(host.view(np.int32)).cuda()

@@ -73,10 +73,10 @@ def test_d_batched_device_api(M, orc):
     for b in range(batch):
         er, ei = f(xr[b], xi[b])
         assert _bits_equal(yr[b], er) and _bits_equal(yi[b], ei)
-    # device layout [c][p][b]
-    d_in = torch.from_numpy(np.stack([xr.T, xi.T]).copy()).cuda()
+    # device layout [c][b][p]
+    d_in = torch.from_numpy(np.stack([xr, xi]).copy()).cuda()
     d_out = torch.empty_like(d_in)
     plan.execute_device(batch, d_in.data_ptr(), d_out.data_ptr(), stream=torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     out = d_out.cpu().numpy()
-    assert _bits_equal(out[0].T, yr) and _bits_equal(out[1].T, yi)
+    assert _bits_equal(out[0], yr) and _bits_equal(out[1], yi)
