@@ -221,6 +221,7 @@ def main():
 
     import mpfft_b200 as M
     from mpfft_b200 import mparray
+    from mpfft_b200.dist import max_over_ranks, rank_seed
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -232,7 +233,7 @@ def main():
     plan = M.MpPlan(n, p)
     L = plan.limbs
     xr, xi = mparray.MpfrArray(n * B, p), mparray.MpfrArray(n * B, p)
-    mparray.fill_uniform(xr, xi, SEED + rank)
+    mparray.fill_uniform(xr, xi, rank_seed(SEED, rank))
     import numpy as np
 
     host = np.zeros(plan.words(B), dtype=np.uint32)
@@ -269,11 +270,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(e0.elapsed_time(e1), device="cuda")
     value = args.steps * B * world / (ms_max / 1e3)
     sched = plan.schedule()
     launches_per_step = 1 + len(sched)
@@ -324,11 +321,8 @@ def main():
     for _ in range(e2e_steps):
         plan.execute(B, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
     torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
-    tt = torch.tensor([dt], device="cuda")
-    if world > 1:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e = e2e_steps * B * world / float(tt.item())
+    dt = max_over_ranks(time.perf_counter() - t0, device="cuda")
+    e2e = e2e_steps * B * world / dt
 
     # ---- accuracy of signal 0 against the 2P-bit oracle (CPU baseline leg) ----
     acc = {}

@@ -51,6 +51,7 @@ extern "C" {
 
 /* flags */
 #define MPFFT_SCALED 1u         /* execute: multiply the result by 1/n (exact) */
+#define MPFFT_INVERSE 8u        /* execute (host arrays): backward transform, exp(+2 pi i jk/n) */
 #define MPFFT_PLAN_HOST_ONLY 2u /* plan creation: conversion (pack/unpack) only, no device state */
 #define MPFFT_PLAN_HOST_CONVERSION 4u /* plan creation: convert mpfr_t <-> limbs on the host, not the GPU */
 
@@ -76,6 +77,14 @@ void mp_sr24_cp_fft_v2(unsigned long n, unsigned long log2n, unsigned long s, lo
 void mp_sr24_cp_fft_scaled(unsigned long n, unsigned long s, long int sn, mpfr_t *inr, mpfr_t *ini,
                            mpfr_t *outr, mpfr_t *outi);
 
+/* Inverse transform, normalised: out = (1/n) sum_k in[k] exp(+2 pi i jk/n).  The
+ * reference computes its inverse in test() as swap(re,im), forward transform,
+ * swap back, divide by N (lab/parallel/mp/parallel_mp_fft2.c:441-455); this is
+ * that procedure with the re/im swap done by addressing (no copies) and the
+ * 1/n applied exactly before the single rounding into each output. */
+void mp_sr24_cp_ifft(unsigned long n, unsigned long s, long int sn, mpfr_t *inr, mpfr_t *ini, mpfr_t *outr,
+                     mpfr_t *outi);
+
 /* Replaces d_sr24_cp_fft, mpFFT.h:25,53 (lab/serial/double/serial_d_fft6.c:93-429).
  * Results are bit-identical to the reference's double transform. */
 void d_sr24_cp_fft(unsigned long n, unsigned long s, long int sn, double *inr, double *ini, double *outr,
@@ -84,6 +93,11 @@ void d_sr24_cp_fft(unsigned long n, unsigned long s, long int sn, double *inr, d
 /* Replaces d_sr24_cp_fft_v2, mpFFT.h:26 (lab/serial/double/serial_d_fft7.c:93-94). */
 void d_sr24_cp_fft_v2(unsigned long n, unsigned long log2n, unsigned long s, long int sn, double *inr,
                       double *ini, double *outr, double *outi);
+
+/* FP64 inverse, normalised; bit-identical to the reference's swap / forward /
+ * swap / divide-by-N procedure (lab/serial/double/serial_d_fft6.c:511-524). */
+void d_sr24_cp_ifft(unsigned long n, unsigned long s, long int sn, double *inr, double *ini, double *outr,
+                    double *outi);
 
 /* FP64 scaled variant: out = FFT(in) * (1/n), exact power-of-two scaling. */
 void d_sr24_cp_fft_scaled(unsigned long n, unsigned long s, long int sn, double *inr, double *ini,

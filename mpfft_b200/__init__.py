@@ -27,6 +27,7 @@ OK, EINVAL, EUNSUPPORTED, ENONFINITE, ECUDA, ENOMEM = 0, 1, 2, 3, 4, 5
 SCALED = 1
 PLAN_HOST_ONLY = 2
 PLAN_HOST_CONVERSION = 4
+INVERSE = 8
 
 
 class MpfftError(RuntimeError):
@@ -52,6 +53,8 @@ def _load() -> C.CDLL:
         "mp_sr24_cp_fft": (None, [ul, ul, sl, vp, vp, vp, vp]),
         "mp_sr24_cp_fft_v2": (None, [ul, ul, ul, sl, vp, vp, vp, vp]),
         "mp_sr24_cp_fft_scaled": (None, [ul, ul, sl, vp, vp, vp, vp]),
+        "mp_sr24_cp_ifft": (None, [ul, ul, sl, vp, vp, vp, vp]),
+        "d_sr24_cp_ifft": (None, [ul, ul, sl, dp, dp, dp, dp]),
         "d_sr24_cp_fft": (None, [ul, ul, sl, dp, dp, dp, dp]),
         "d_sr24_cp_fft_v2": (None, [ul, ul, ul, sl, dp, dp, dp, dp]),
         "d_sr24_cp_fft_scaled": (None, [ul, ul, sl, dp, dp, dp, dp]),
@@ -122,6 +125,11 @@ def mp_sr24_cp_fft_scaled(n, s, sn, inr, ini, outr, outi) -> int:
     return lib.mpfft_last_error()
 
 
+def mp_sr24_cp_ifft(n, s, sn, inr, ini, outr, outi) -> int:
+    lib.mp_sr24_cp_ifft(n, s, sn, inr, ini, outr, outi)
+    return lib.mpfft_last_error()
+
+
 def _dp(a):
     return a.ctypes.data_as(C.c_void_p) if hasattr(a, "ctypes") else a
 
@@ -133,6 +141,11 @@ def d_sr24_cp_fft(n, s, sn, inr, ini, outr, outi) -> int:
 
 def d_sr24_cp_fft_v2(n, log2n, s, sn, inr, ini, outr, outi) -> int:
     lib.d_sr24_cp_fft_v2(n, log2n, s, sn, _dp(inr), _dp(ini), _dp(outr), _dp(outi))
+    return lib.mpfft_last_error()
+
+
+def d_sr24_cp_ifft(n, s, sn, inr, ini, outr, outi) -> int:
+    lib.d_sr24_cp_ifft(n, s, sn, _dp(inr), _dp(ini), _dp(outr), _dp(outi))
     return lib.mpfft_last_error()
 
 
@@ -168,8 +181,9 @@ class MpPlan:
         """32-bit words of one limb-plane buffer holding `batch` signals."""
         return 2 * self.limbs * self.n * batch
 
-    def execute(self, batch, inr, ini, outr, outi, scaled=False) -> None:
-        _check(lib.mpfft_mp_execute(self.h, batch, inr, ini, outr, outi, SCALED if scaled else 0))
+    def execute(self, batch, inr, ini, outr, outi, scaled=False, inverse=False) -> None:
+        flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
+        _check(lib.mpfft_mp_execute(self.h, batch, inr, ini, outr, outi, flags))
 
     def execute_device(self, batch, d_in: int, d_out: int, stream: int = 0) -> None:
         _check(lib.mpfft_mp_execute_device(self.h, batch, d_in, d_out, stream or None))
@@ -225,9 +239,9 @@ class DPlan:
 
     __del__ = close
 
-    def execute(self, batch, inr, ini, outr, outi, scaled=False) -> None:
-        _check(lib.mpfft_d_execute(self.h, batch, _dp(inr), _dp(ini), _dp(outr), _dp(outi),
-                                   SCALED if scaled else 0))
+    def execute(self, batch, inr, ini, outr, outi, scaled=False, inverse=False) -> None:
+        flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
+        _check(lib.mpfft_d_execute(self.h, batch, _dp(inr), _dp(ini), _dp(outr), _dp(outi), flags))
 
     def execute_device(self, batch, d_in: int, d_out: int, scaled=False, stream: int = 0) -> None:
         _check(lib.mpfft_d_execute_device(self.h, batch, d_in, d_out, SCALED if scaled else 0, stream or None))

@@ -96,7 +96,7 @@ __global__ void mp_export(const uint32_t *__restrict__ planes, int N, int B, int
   const int p = (int)(cp - (long long)c * N);
   const size_t plane = (size_t)N * B;
   const uint32_t *src = planes + ((size_t)c * L * N + p) * B + b;
-  uint64_t a[(kMaxLimbs + 2) / 2 + 1];  // magnitude in 64-bit limbs
+  uint64_t a[(kMaxLimbsBig + 2) / 2 + 1];  // magnitude in 64-bit limbs
   const int na = (L + 1) / 2;
   const bool neg = (src[(size_t)(L - 1) * plane] >> 31) != 0;
   {

@@ -169,7 +169,7 @@ static uint32_t mpfr_to_fixed(mpfr_srcptr x, int L, long F, long e_s, uint32_t *
 
 // two's-complement L-word integer A -> y = A * 2^e2, rounded to y's precision.
 static void fixed_to_mpfr(const uint32_t *A, int L, long e2, mpfr_ptr y) {
-  uint32_t mag[80];
+  uint32_t mag[kMaxLimbsBig + 2];
   const bool neg = (A[L - 1] >> 31) != 0;
   uint32_t c = neg ? 1u : 0u;
   const uint32_t m = neg ? 0xffffffffu : 0u;
@@ -248,7 +248,7 @@ static int build_twiddles(MpTwiddles &tw, unsigned long N, int L) {
     mpfr_init2(c, pw);
     mpfr_init2(t, pw);
     mpfr_const_pi(pi2, MPFR_RNDN);
-    uint32_t tmp[80];
+    uint32_t tmp[kMaxLimbsBig + 2];
     for (long k = a; k < b; ++k) {
       mpfr_mul_ui(th, pi2, 2UL * (unsigned long)k, MPFR_RNDN);
       mpfr_div_ui(th, th, N, MPFR_RNDN);
@@ -287,6 +287,8 @@ struct mpfft_mp_plan {
   long F = 0;  // fraction bits
   bool host_only = false;  // conversion-only plan: no device state
   bool force_host_conversion = false;  // convert mpfr_t <-> limbs on the host even when the GPU could
+  uint32_t *d_big = nullptr;  // streaming-kernel scratch (L > kMaxLimbs), grown on demand
+  size_t big_words = 0;
   DeviceTree tree;
   MpTwiddles tw;
   MpDeviceTables tabs;
@@ -306,6 +308,7 @@ struct mpfft_mp_plan {
     uint64_t *h_mi = nullptr, *d_mi = nullptr, *h_mo = nullptr, *d_mo = nullptr;
     int64_t *h_ei = nullptr, *d_ei = nullptr, *h_eo = nullptr, *d_eo = nullptr, *d_es = nullptr;
     uint8_t *h_si = nullptr, *d_si = nullptr, *h_so = nullptr, *d_so = nullptr;
+    uint32_t *d_big = nullptr;  // streaming-kernel scratch of this slot (L > kMaxLimbs)
   };
   ConvSlot cv[2];
   unsigned long cv_chunk = 0;  // signals per chunk the slots hold
@@ -313,7 +316,7 @@ struct mpfft_mp_plan {
   void free_conv() {
     for (auto &c : cv) {
       for (void *q : {(void *)c.d_in, (void *)c.d_out, (void *)c.d_mi, (void *)c.d_mo, (void *)c.d_ei,
-                      (void *)c.d_eo, (void *)c.d_es, (void *)c.d_si, (void *)c.d_so})
+                      (void *)c.d_eo, (void *)c.d_es, (void *)c.d_si, (void *)c.d_so, (void *)c.d_big})
         if (q) cudaFree(q);
       for (void *q : {(void *)c.h_mi, (void *)c.h_mo, (void *)c.h_ei, (void *)c.h_eo, (void *)c.h_si, (void *)c.h_so})
         if (q) cudaFreeHost(q);
@@ -325,6 +328,7 @@ struct mpfft_mp_plan {
   }
   ~mpfft_mp_plan() {
     free_conv();
+    if (d_big) cudaFree(d_big);
     if (d_in) cudaFree(d_in);
     if (d_out) cudaFree(d_out);
     if (h_in) cudaFreeHost(h_in);
@@ -370,9 +374,9 @@ static int mp_plan_init(mpfft_mp_plan *p, unsigned long n, long prec, bool host_
   if (prec < 2) return set_err(MPFFT_EINVAL, "precision %ld < 2", prec);
   if (n > (1UL << 26)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
   int L = mp_limbs_for(n, prec);
-  if (L > kMaxLimbs)
+  if (L > kMaxLimbsBig)
     return set_err(MPFFT_EUNSUPPORTED, "precision %ld at n=%lu needs %d limbs (> %d supported)", prec, n, L,
-                   kMaxLimbs);
+                   kMaxLimbsBig);
   p->N = n;
   p->P = prec;
   p->L = L;
@@ -453,7 +457,7 @@ static int mp_pack_impl(const mpfft_mp_plan *P, unsigned long batch, mpfr_t *inr
     if (bad[b]) return set_err(MPFFT_ENONFINITE, "input signal %lu holds NaN or infinity", b);
   const size_t plane = (size_t)N * batch;
   parallel_for((long)(N * batch), 256, [&](long a0, long a1) {
-    uint32_t tmp[80];
+    uint32_t tmp[kMaxLimbsBig + 2];
     for (long t = a0; t < a1; ++t) {
       const unsigned long p = t / batch, b = t % batch;
       for (int c = 0; c < 2; ++c) {
@@ -481,7 +485,7 @@ static void mp_unpack_impl(const mpfft_mp_plan *P, unsigned long batch, const ui
   const size_t plane = (size_t)N * batch;
   const long shift = (flags & MPFFT_SCALED) ? ilog2(N) : 0;
   parallel_for((long)(N * batch), 256, [&](long a0, long a1) {
-    uint32_t tmp[80];
+    uint32_t tmp[kMaxLimbsBig + 2];
     for (long t = a0; t < a1; ++t) {
       const unsigned long p = t / batch, b = t % batch;
       for (int c = 0; c < 2; ++c) {
@@ -524,6 +528,7 @@ static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int n
     dm((void **)&c.d_so, comp);
     hm((void **)&c.h_so, comp);
     dm((void **)&c.d_es, chunk * 8);
+    if (p->L > kMaxLimbs) dm((void **)&c.d_big, mp_big_scratch_words(p->tabs, p->L, (int)chunk) * 4);
   }
   if (!ok) {
     cudaGetLastError();
@@ -602,7 +607,7 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr
     CUDA_TRY(cudaMemcpyAsync(c.d_ei, c.h_ei, comp * 8, cudaMemcpyHostToDevice, c.st));
     CUDA_TRY(cudaMemcpyAsync(c.d_si, c.h_si, comp, cudaMemcpyHostToDevice, c.st));
     CUDA_TRY(mp_import_launch(c.d_mi, c.d_ei, c.d_si, nli, (int)N, (int)cb, p->L, p->F, c.d_es, c.d_in, c.st));
-    CUDA_TRY(mp_run_transform(p->L, p->tabs, c.d_in, c.d_out, (int)cb, c.st));
+    CUDA_TRY(mp_run_transform(p->L, p->tabs, c.d_in, c.d_out, (int)cb, c.st, nullptr, c.d_big));
     CUDA_TRY(mp_export_launch(c.d_out, (int)N, (int)cb, p->L, c.d_es, p->F + shift, prec_out, nlo, c.d_mo, c.d_eo,
                               c.d_so, c.st));
     CUDA_TRY(cudaMemcpyAsync(c.h_mo, c.d_mo, comp * nlo * 8, cudaMemcpyDeviceToHost, c.st));
@@ -660,6 +665,25 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr
   return set_err(MPFFT_OK, "");
 }
 
+// streaming-kernel scratch for a batch (large limb counts only); null otherwise
+static int mp_big_reserve(mpfft_mp_plan *p, unsigned long batch, uint32_t **out) {
+  *out = nullptr;
+  if (p->L <= kMaxLimbs) return MPFFT_OK;
+  const size_t words = mp_big_scratch_words(p->tabs, p->L, (int)batch);
+  if (words > p->big_words) {
+    if (p->d_big) cudaFree(p->d_big);
+    p->d_big = nullptr;
+    p->big_words = 0;
+    if (cudaMalloc(&p->d_big, words * 4) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(MPFFT_ENOMEM, "cannot allocate %zu bytes of scratch", words * 4);
+    }
+    p->big_words = words;
+  }
+  *out = p->d_big;
+  return MPFFT_OK;
+}
+
 static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr, mpfr_t *ini, unsigned long s,
                            mpfr_t *outr, mpfr_t *outi, unsigned flags) {
   if (p->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
@@ -672,8 +696,10 @@ static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr, m
   p->exps.assign(batch, 0);
   if (int e = mp_pack_impl(p, batch, inr, ini, s, p->h_in, p->exps.data())) return e;
   const size_t bytes = (size_t)2 * p->L * p->N * batch * 4;
+  uint32_t *big = nullptr;
+  if (int e = mp_big_reserve(p, batch, &big)) return e;
   CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, bytes, cudaMemcpyHostToDevice, p->stream));
-  CUDA_TRY(mp_run_transform(p->L, p->tabs, p->d_in, p->d_out, (int)batch, p->stream));
+  CUDA_TRY(mp_run_transform(p->L, p->tabs, p->d_in, p->d_out, (int)batch, p->stream, nullptr, big));
   CUDA_TRY(cudaMemcpyAsync(p->h_out, p->d_out, bytes, cudaMemcpyDeviceToHost, p->stream));
   CUDA_TRY(cudaStreamSynchronize(p->stream));
   mp_unpack_impl(p, batch, p->h_out, p->exps.data(), outr, outi, flags);
@@ -693,6 +719,11 @@ static void mp_dropin(unsigned long n, unsigned long s, long sn, mpfr_t *inr, mp
   if (!inr || !ini || !outr || !outi) {
     set_err(MPFFT_EINVAL, "NULL array");
     return;
+  }
+  if (flags & MPFFT_INVERSE) {  // ifft(X) = swap(FFT(swap(X))) (times 1/n if scaled)
+    std::swap(inr, ini);
+    std::swap(outr, outi);
+    flags &= ~MPFFT_INVERSE;
   }
   int e = MPFFT_OK;
   if (!is_pow2(n)) e = set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
@@ -865,6 +896,11 @@ static void d_dropin(unsigned long n, unsigned long s, long sn, double *inr, dou
     set_err(MPFFT_EINVAL, "NULL array");
     return;
   }
+  if (flags & MPFFT_INVERSE) {  // ifft(X) = swap(FFT(swap(X))) (times 1/n if scaled)
+    std::swap(inr, ini);
+    std::swap(outr, outi);
+    flags &= ~MPFFT_INVERSE;
+  }
   int e = MPFFT_OK;
   if (!is_pow2(n)) e = set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
   else if (s == 0) e = set_err(MPFFT_EINVAL, "stride s must be >= 1");
@@ -907,6 +943,16 @@ MPFFT_API void mp_sr24_cp_fft_v2(unsigned long n, unsigned long log2n, unsigned 
 MPFFT_API void mp_sr24_cp_fft_scaled(unsigned long n, unsigned long s, long sn, mpfr_t *inr, mpfr_t *ini,
                                      mpfr_t *outr, mpfr_t *outi) {
   mp_dropin(n, s, sn, inr, ini, outr, outi, MPFFT_SCALED);
+}
+
+MPFFT_API void mp_sr24_cp_ifft(unsigned long n, unsigned long s, long sn, mpfr_t *inr, mpfr_t *ini, mpfr_t *outr,
+                               mpfr_t *outi) {
+  mp_dropin(n, s, sn, inr, ini, outr, outi, MPFFT_INVERSE | MPFFT_SCALED);
+}
+
+MPFFT_API void d_sr24_cp_ifft(unsigned long n, unsigned long s, long sn, double *inr, double *ini, double *outr,
+                              double *outi) {
+  d_dropin(n, s, sn, inr, ini, outr, outi, MPFFT_INVERSE | MPFFT_SCALED);
 }
 
 MPFFT_API void d_sr24_cp_fft(unsigned long n, unsigned long s, long sn, double *inr, double *ini, double *outr,
@@ -960,6 +1006,11 @@ MPFFT_API int mpfft_mp_execute(mpfft_mp_plan *plan, unsigned long batch, mpfr_t 
                                mpfr_t *outi, unsigned flags) {
   if (!plan || !inr || !ini || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
   if (batch == 0) return set_err(MPFFT_OK, "");
+  if (flags & MPFFT_INVERSE) {  // ifft(X) = swap(FFT(swap(X))) (times 1/n if scaled)
+    std::swap(inr, ini);
+    std::swap(outr, outi);
+    flags &= ~MPFFT_INVERSE;
+  }
   int e = mp_execute_impl(plan, batch, inr, ini, 1, outr, outi, flags);
   if (e != MPFFT_OK) {
     mp_fill_nan(outr, plan->N * batch);
@@ -977,7 +1028,9 @@ MPFFT_API int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, 
   const char *a = (const char *)d_in, *b = (const char *)d_out;
   if (a < b + bytes && b < a + bytes) return set_err(MPFFT_EINVAL, "input and output buffers overlap");
   if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");
-  CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream));
+  uint32_t *big = nullptr;
+  if (int e = mp_big_reserve(plan, batch, &big)) return e;
+  CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream, nullptr, big));
   return set_err(MPFFT_OK, "");
 }
 
@@ -1014,6 +1067,11 @@ MPFFT_API int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const dou
                               double *outr, double *outi, unsigned flags) {
   if (!plan || !inr || !ini || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
   if (batch == 0) return set_err(MPFFT_OK, "");
+  if (flags & MPFFT_INVERSE) {  // ifft(X) = swap(FFT(swap(X))) (times 1/n if scaled)
+    std::swap(inr, ini);
+    std::swap(outr, outi);
+    flags &= ~MPFFT_INVERSE;
+  }
   return d_execute_impl(plan, batch, inr, ini, 1, outr, outi, flags);
 }
 
@@ -1046,7 +1104,9 @@ MPFFT_API int mpfft_mp_execute_device_timed(mpfft_mp_plan *plan, unsigned long b
                                             uint32_t *d_out, void *stream, float *launch_ms) {
   if (!plan || !d_in || !d_out || !launch_ms) return set_err(MPFFT_EINVAL, "NULL argument");
   if (plan->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
-  CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream, launch_ms));
+  uint32_t *big = nullptr;
+  if (int e = mp_big_reserve(plan, batch, &big)) return e;
+  CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream, launch_ms, big));
   return set_err(MPFFT_OK, "");
 }
 
@@ -1072,6 +1132,9 @@ MPFFT_API int mpfft_mp_execute_significands_static(const mpfft_mp_plan *plan, un
   if (nl_in < 1 || prec_out < 2) return set_err(MPFFT_EINVAL, "nl_in must be >= 1 and prec_out >= 2");
   if (batch == 0) return set_err(MPFFT_OK, "");
   if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  if (plan->L > kMaxLimbs)
+    return set_err(MPFFT_EUNSUPPORTED, "the static-scratch entry point supports up to %d limbs (plan has %d)",
+                   kMaxLimbs, plan->L);
   MpPlanView v;
   v.N = plan->N;
   v.L = plan->L;

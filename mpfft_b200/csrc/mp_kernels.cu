@@ -247,35 +247,6 @@ __global__ void __launch_bounds__(128, 4) mp_level_kernel(uint32_t *__restrict__
 // host-side launchers, one instantiation per supported limb count
 // ---------------------------------------------------------------------------
 
-// Optional per-launch timing with events on the launch stream.
-struct LaunchTimer {
-  float *ms;
-  cudaStream_t s;
-  cudaEvent_t ev[2 * (kMaxLevels + 1)] = {};
-  int n = 0;
-  LaunchTimer(float *ms_, cudaStream_t s_) : ms(ms_), s(s_) {}
-  void begin() {
-    if (!ms) return;
-    cudaEventCreate(&ev[2 * n]);
-    cudaEventCreate(&ev[2 * n + 1]);
-    cudaEventRecord(ev[2 * n], s);
-  }
-  void end() {
-    if (!ms) return;
-    cudaEventRecord(ev[2 * n + 1], s);
-    ++n;
-  }
-  ~LaunchTimer() {
-    if (!ms) return;
-    cudaStreamSynchronize(s);
-    for (int i = 0; i < n; ++i) {
-      cudaEventElapsedTime(&ms[i], ev[2 * i], ev[2 * i + 1]);
-      cudaEventDestroy(ev[2 * i]);
-      cudaEventDestroy(ev[2 * i + 1]);
-    }
-  }
-};
-
 template <int L>
 static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
                                  cudaStream_t s, float *launch_ms) {
@@ -306,7 +277,11 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
     return run_transform<LL>(T, in, out, B, s, launch_ms);
 
 cudaError_t mp_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
-                             cudaStream_t s, float *launch_ms) {
+                             cudaStream_t s, float *launch_ms, uint32_t *big_scratch) {
+  if (L > kMaxLimbs) {
+    if (!big_scratch || L > kMaxLimbsBig) return cudaErrorInvalidValue;
+    return mp_big_run_transform(L, T, in, out, B, big_scratch, s, launch_ms);
+  }
   switch (L) {
     MPFFT_MP_CASE(2) MPFFT_MP_CASE(3) MPFFT_MP_CASE(4) MPFFT_MP_CASE(5) MPFFT_MP_CASE(6) MPFFT_MP_CASE(7)
     MPFFT_MP_CASE(8) MPFFT_MP_CASE(9) MPFFT_MP_CASE(10) MPFFT_MP_CASE(11) MPFFT_MP_CASE(12)

@@ -88,15 +88,51 @@ struct MpPlanView {
   const MpDeviceTables *tabs = nullptr;
 };
 
-// largest limb count with register-resident kernels
+// largest limb count with register-resident kernels; above it (up to
+// kMaxLimbsBig) the streaming kernels of mp_big_kernels.cu run
 constexpr int kMaxLimbs = 34;
+constexpr int kMaxLimbsBig = 520;
 constexpr int kMinLimbs = 2;
 
 // launch_ms (optional, host array of >= 1 + nlevels floats): when non-null,
 // each launch is bracketed by events on `s` and its duration written there
 // (the call then synchronizes); used by benchmarks to attribute time.
+// Optional per-launch timing with events on the launch stream.
+struct LaunchTimer {
+  float *ms;
+  cudaStream_t s;
+  cudaEvent_t ev[2 * (kMaxLevels + 1)] = {};
+  int n = 0;
+  LaunchTimer(float *ms_, cudaStream_t s_) : ms(ms_), s(s_) {}
+  void begin() {
+    if (!ms) return;
+    cudaEventCreate(&ev[2 * n]);
+    cudaEventCreate(&ev[2 * n + 1]);
+    cudaEventRecord(ev[2 * n], s);
+  }
+  void end() {
+    if (!ms) return;
+    cudaEventRecord(ev[2 * n + 1], s);
+    ++n;
+  }
+  ~LaunchTimer() {
+    if (!ms) return;
+    cudaStreamSynchronize(s);
+    for (int i = 0; i < n; ++i) {
+      cudaEventElapsedTime(&ms[i], ev[2 * i], ev[2 * i + 1]);
+      cudaEventDestroy(ev[2 * i]);
+      cudaEventDestroy(ev[2 * i + 1]);
+    }
+  }
+};
+
+// big_scratch: device buffer of mp_big_scratch_words(T, L, B) words, needed
+// (and only used) when L > kMaxLimbs.
 cudaError_t mp_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
-                             cudaStream_t s, float *launch_ms = nullptr);
+                             cudaStream_t s, float *launch_ms = nullptr, uint32_t *big_scratch = nullptr);
+size_t mp_big_scratch_words(const MpDeviceTables &T, int L, int B);
+cudaError_t mp_big_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
+                                 uint32_t *scratch, cudaStream_t s, float *launch_ms);
 cudaError_t diag_imad_rate(int wide, double *ops_per_s);
 
 // GPU-side conversion between MPFR significands and limb planes.  Component

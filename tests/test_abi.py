@@ -38,9 +38,10 @@ def test_limb_format(M, n, p, limbs):
     assert pl.frac_bits >= p + lg + 4
 
 
-def test_precision_beyond_register_kernels_is_reported(M):
+def test_precision_beyond_supported_limbs_is_reported(M):
+    assert M.MpPlan(1024, 8192, host_only=True).limbs == 257
     with pytest.raises(M.MpfftError) as e:
-        M.MpPlan(1024, 4096, host_only=True)
+        M.MpPlan(1024, 20000, host_only=True)
     assert e.value.code == M.EUNSUPPORTED
 
 

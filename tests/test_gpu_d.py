@@ -80,3 +80,21 @@ def test_d_batched_device_api(M, orc):
     torch.cuda.synchronize()
     out = d_out.cpu().numpy()
     assert _bits_equal(out[0], yr) and _bits_equal(out[1], yi)
+
+
+@pytest.mark.parametrize("n", [1, 16, 1024, 65536])
+def test_d_inverse_bitexact_vs_reference_procedure(M, orc, n):
+    """d_sr24_cp_ifft is bit-identical to the reference's test() inverse:
+    swap re/im, forward transform, swap back, divide by N
+    (lab/serial/double/serial_d_fft6.c:511-524)."""
+    O = orc
+    xr, xi = O.d_uniform(n, 900 + n)
+    fr, fi = O.DFFT(n)(xi, xr)           # forward of the swapped input
+    er, ei = fi / n, fr / n              # swap back, divide by N
+    yr, yi = np.zeros(n), np.zeros(n)
+    assert M.d_sr24_cp_ifft(n, 1, 0, xr, xi, yr, yi) == M.OK
+    assert _bits_equal(yr, er) and _bits_equal(yi, ei)
+    plan = M.DPlan(n)
+    zr, zi = np.zeros(n), np.zeros(n)
+    plan.execute(1, xr, xi, zr, zi, scaled=True, inverse=True)
+    assert _bits_equal(zr, er) and _bits_equal(zi, ei)

@@ -227,3 +227,61 @@ def test_mp_gpu_conversion_matches_host_conversion(M, orc, n, p_in, p_out, batch
     host.execute(batch, xr.ptr, xi.ptr, zr.ptr, zi.ptr, scaled=scaled)
     assert L.orc_mp_count_diff(yr.ptr, zr.ptr, n * batch) == 0
     assert L.orc_mp_count_diff(yi.ptr, zi.ptr, n * batch) == 0
+
+
+@pytest.mark.parametrize("n,p", [(256, 256), (1024, 1024), (4, 64)])
+def test_mp_inverse_entry(M, orc, n, p):
+    """mp_sr24_cp_ifft = the reference's test() inverse (swap, forward, swap,
+    divide by N); against the 2P-bit inverse DFT and as a round trip."""
+    O = orc
+    L = O.lib()
+    xr, xi = _inputs(O, n, p, 41)
+    yr, yi = O.mp_pair(n, p)
+    assert M.mp_sr24_cp_ifft(n, 1, 0, xr.ptr, xi.ptr, yr.ptr, yi.ptr) == M.OK
+    # 2P oracle of the inverse: (1/n) swap(DFT(swap(x)))
+    dr, di = O.mp_pair(n, 2 * p)
+    O.mp_dft(xi, xr, di, dr)
+    L.orc_mp_scale2(dr.ptr, n, -int(math.log2(n)))
+    L.orc_mp_scale2(di.ptr, n, -int(math.log2(n)))
+    assert O.mp_errors(yr, yi, dr, di)["log2_rel"] <= O.mp_bound_log2(n, p)
+    # forward of the inverse returns the input
+    zr, zi = O.mp_pair(n, p)
+    assert M.mp_sr24_cp_fft(n, 1, 0, yr.ptr, yi.ptr, zr.ptr, zi.ptr) == M.OK
+    assert O.mp_errors(zr, zi, xr, xi)["log2_rel"] <= O.mp_bound_log2(n, p) + 1
+    # batched flag gives the same result
+    plan = M.MpPlan(n, p)
+    wr, wi = O.mp_pair(n, p)
+    plan.execute(1, xr.ptr, xi.ptr, wr.ptr, wi.ptr, scaled=True, inverse=True)
+    assert L.orc_mp_count_diff(wr.ptr, yr.ptr, n) == 0 and L.orc_mp_count_diff(wi.ptr, yi.ptr, n) == 0
+
+
+@pytest.mark.parametrize("n,p,batch", [(16, 2048, 1), (64, 2048, 32), (16, 4096, 2), (8, 8192, 1), (256, 1100, 1)])
+def test_mp_large_precision(M, orc, n, p, batch):
+    """Precisions beyond the register kernels (L > 34 limbs) run the streaming
+    kernels: same error bound against the 2P-bit DFT, no worse than the
+    reference at the same P; host-array, batched and conversion paths agree."""
+    O = orc
+    L = O.lib()
+    xr, xi = O.mp_pair(n * batch, p)
+    O.fill_uniform(xr, xi, 55 + p)
+    plan = M.MpPlan(n, p)
+    assert plan.limbs > 34
+    yr, yi = O.mp_pair(n * batch, p)
+    plan.execute(batch, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
+    zr, zi = O.mp_pair(n * batch, p)
+    M.MpPlan(n, p, host_conversion=True).execute(batch, xr.ptr, xi.ptr, zr.ptr, zi.ptr)
+    assert L.orc_mp_count_diff(yr.ptr, zr.ptr, n * batch) == 0 and L.orc_mp_count_diff(yi.ptr, zi.ptr, n * batch) == 0
+    for b in (0, batch - 1):
+        sr, si = O.mp_pair(n, p)
+        L.orc_mp_copy(sr.ptr, xr.ptr + b * n * 32, n)
+        L.orc_mp_copy(si.ptr, xi.ptr + b * n * 32, n)
+        gr, gi = O.mp_pair(n, p)
+        L.orc_mp_copy(gr.ptr, yr.ptr + b * n * 32, n)
+        L.orc_mp_copy(gi.ptr, yi.ptr + b * n * 32, n)
+        dr, di = O.mp_pair(n, 2 * p)
+        O.mp_dft(sr, si, dr, di)
+        e_gpu = O.mp_errors(gr, gi, dr, di)["log2_rel"]
+        rr, ri = O.mp_pair(n, p)
+        O.MpFFT(n, p)(sr, si, rr, ri)
+        e_ref = O.mp_errors(rr, ri, dr, di)["log2_rel"]
+        assert e_gpu <= O.mp_bound_log2(n, p) and e_gpu <= e_ref + 0.5, (e_gpu, e_ref)
