@@ -143,6 +143,28 @@ int mpfft_mp_execute(mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr
 int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, const uint32_t *d_in, uint32_t *d_out,
                             void *stream);
 
+/* Real transforms (no counterpart in the reference, whose README lists
+ * "only complex input"; a real signal there is a complex one with zero
+ * imaginary parts).  A real plan for n real points (n a power of two, n >= 2)
+ * runs one n/2-point complex transform plus one split step, about half the
+ * work of the complex transform of the zero-padded signal.  The limb format
+ * (mpfft_mp_plan_limbs/frac_bits) is that of an n-point complex plan, with up
+ * to 34 limbs.  MPFFT_PLAN_HOST_CONVERSION is accepted; real plans have no
+ * device-layout, pack/unpack or static-scratch entry points. */
+int mpfft_mp_plan_create_real(mpfft_mp_plan **plan, unsigned long n, long prec, unsigned flags);
+/* X_k = sum_j x_j exp(-2 pi i jk/n) for k = 0..n/2 of `batch` real signals:
+ * signal b at in[b*n .. b*n+n-1], outputs at outr/outi[b*(n/2+1) + k]
+ * (X_0 and X_(n/2) have zero imaginary parts).  MPFFT_SCALED: times 1/n.
+ * Error bound and rounding as mpfft_mp_execute. */
+int mpfft_mp_execute_r2c(mpfft_mp_plan *plan, unsigned long batch, mpfr_t *in, mpfr_t *outr, mpfr_t *outi,
+                         unsigned flags);
+/* Inverse: x_j = sum_(k<n) X_k exp(+2 pi i jk/n) with X_(n-k) = conj(X_k), from
+ * the half spectrum inr/ini[b*(n/2+1) + k], k = 0..n/2, into out[b*n + j]
+ * (MPFFT_SCALED: times 1/n, the exact inverse of mpfft_mp_execute_r2c).  The
+ * imaginary parts of X_0 and X_(n/2) are ignored. */
+int mpfft_mp_execute_c2r(mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr_t *ini, mpfr_t *out,
+                         unsigned flags);
+
 /* Host-side conversion between mpfr_t arrays and the limb-plane layout
  * above.  exps[b] receives (pack) / supplies (unpack) the block exponent of
  * signal b: a component with fixed-point integer A has value

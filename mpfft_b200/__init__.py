@@ -67,6 +67,9 @@ def _load() -> C.CDLL:
         "mpfft_mp_plan_frac_bits": (C.c_long, [vp]),
         "mpfft_mp_execute": (C.c_int, [vp, ul, vp, vp, vp, vp, C.c_uint]),
         "mpfft_mp_execute_device": (C.c_int, [vp, ul, u32p, u32p, vp]),
+        "mpfft_mp_plan_create_real": (C.c_int, [C.POINTER(vp), ul, sl, C.c_uint]),
+        "mpfft_mp_execute_r2c": (C.c_int, [vp, ul, vp, vp, vp, C.c_uint]),
+        "mpfft_mp_execute_c2r": (C.c_int, [vp, ul, vp, vp, vp, C.c_uint]),
         "mpfft_mp_pack": (C.c_int, [vp, ul, vp, vp, u32p, vp]),
         "mpfft_mp_unpack": (C.c_int, [vp, ul, u32p, vp, vp, vp, C.c_uint]),
         "mpfft_d_plan_create": (C.c_int, [C.POINTER(vp), ul]),
@@ -214,6 +217,31 @@ class MpPlan:
 
     def unpack(self, batch, planes_ptr, exps_ptr, outr, outi, scaled=False) -> None:
         _check(lib.mpfft_mp_unpack(self.h, batch, planes_ptr, exps_ptr, outr, outi, SCALED if scaled else 0))
+
+
+class MpRealPlan:
+    """Multiprecision real transform of n real points (n/2+1-point half spectrum)."""
+
+    def __init__(self, n: int, prec: int, host_conversion: bool = False):
+        h = C.c_void_p()
+        _check(lib.mpfft_mp_plan_create_real(C.byref(h), n, prec, PLAN_HOST_CONVERSION if host_conversion else 0))
+        self.h = h
+        self.n, self.prec = n, prec
+        self.limbs = lib.mpfft_mp_plan_limbs(h)
+        self.frac_bits = lib.mpfft_mp_plan_frac_bits(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.mpfft_mp_plan_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def r2c(self, batch, x, outr, outi, scaled=False) -> None:
+        _check(lib.mpfft_mp_execute_r2c(self.h, batch, x, outr, outi, SCALED if scaled else 0))
+
+    def c2r(self, batch, inr, ini, x, scaled=False) -> None:
+        _check(lib.mpfft_mp_execute_c2r(self.h, batch, inr, ini, x, SCALED if scaled else 0))
 
 
 def imad_rate(wide: bool = False) -> float:

@@ -287,6 +287,10 @@ struct mpfft_mp_plan {
   long F = 0;  // fraction bits
   bool host_only = false;  // conversion-only plan: no device state
   bool force_host_conversion = false;  // convert mpfr_t <-> limbs on the host even when the GPU could
+  bool real = false;          // real transform of n_real = 2N points: N-point complex transform + split step
+  unsigned long n_real = 0;
+  // points per signal the staging buffers hold (the half spectrum of a real plan has N+1)
+  unsigned long pts_max() const { return real ? N + 1 : N; }
   uint32_t *d_big = nullptr;  // streaming-kernel scratch (L > kMaxLimbs), grown on demand
   size_t big_words = 0;
   DeviceTree tree;
@@ -369,26 +373,36 @@ static int device_ready() {
   return MPFFT_OK;
 }
 
-static int mp_plan_init(mpfft_mp_plan *p, unsigned long n, long prec, bool host_only = false) {
+// real: n real points, planned as an n/2-point complex transform whose limb
+// format (L, F) and twiddle table are those of an n-point transform.
+static int mp_plan_init(mpfft_mp_plan *p, unsigned long n, long prec, bool host_only = false, bool real = false) {
   if (!is_pow2(n)) return set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
+  if (real && n < 2) return set_err(MPFFT_EINVAL, "a real transform needs n >= 2 (n=%lu)", n);
   if (prec < 2) return set_err(MPFFT_EINVAL, "precision %ld < 2", prec);
   if (n > (1UL << 26)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
   int L = mp_limbs_for(n, prec);
   if (L > kMaxLimbsBig)
     return set_err(MPFFT_EUNSUPPORTED, "precision %ld at n=%lu needs %d limbs (> %d supported)", prec, n, L,
                    kMaxLimbsBig);
-  p->N = n;
+  if (real && L > kMaxLimbs)
+    return set_err(MPFFT_EUNSUPPORTED, "real transforms support up to %d limbs (precision %ld at n=%lu needs %d)",
+                   kMaxLimbs, prec, n, L);
+  const unsigned long nt = real ? n / 2 : n;  // complex transform size
+  p->N = nt;
+  p->real = real;
+  p->n_real = real ? n : 0;
   p->P = prec;
   p->L = L;
   p->F = 32L * L - 1 - (ilog2(n) + 2);
   p->host_only = host_only;
   if (host_only) return MPFFT_OK;
   if (int e = device_ready()) return e;
-  if (int e = build_tree(p->tree, n, 4)) return e;
+  if (int e = build_tree(p->tree, nt, 4)) return e;
   if (int e = build_twiddles(p->tw, n, L)) return e;
   static_cast<TreeTables &>(p->tabs) = p->tree.tabs;
   p->tabs.tw = p->tw.d_tw;
   p->tabs.dneg = p->tw.d_dneg;
+  p->tabs.tws = real ? 2 : 1;
   CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   return MPFFT_OK;
 }
@@ -412,7 +426,7 @@ static mpfft_mp_plan *mp_cached(unsigned long n, long prec) {
 }
 
 static int mp_reserve(mpfft_mp_plan *p, unsigned long batch) {
-  const size_t words = (size_t)2 * p->L * p->N * batch;
+  const size_t words = (size_t)2 * p->L * p->pts_max() * batch;
   if (words <= p->cap_words) return MPFFT_OK;
   if (p->d_in) cudaFree(p->d_in);
   if (p->d_out) cudaFree(p->d_out);
@@ -429,14 +443,21 @@ static int mp_reserve(mpfft_mp_plan *p, unsigned long batch) {
   return MPFFT_OK;
 }
 
-// signal b, element p of a strided host array
-static inline mpfr_srcptr elem(mpfr_t *a, unsigned long b, unsigned long N, unsigned long p, unsigned long s) {
-  return a[b * N * s + p * s];
+// Geometry of a host mpfr_t array: element q < n of signal b is a[b*pitch + q*s].
+struct IoShape {
+  unsigned long n, pitch, s;
+};
+static inline IoShape io_signals(unsigned long n, unsigned long s) { return IoShape{n, n * s, s}; }
+static inline mpfr_ptr elem(mpfr_t *a, unsigned long b, const IoShape &io, unsigned long q) {
+  return a[b * io.pitch + q * io.s];
 }
 
-static int mp_pack_impl(const mpfft_mp_plan *P, unsigned long batch, mpfr_t *inr, mpfr_t *ini, unsigned long s,
+// What runs between import and export on the device.
+enum MpMode { kComplex = 0, kR2C = 1, kC2R = 2 };
+
+static int mp_pack_impl(const mpfft_mp_plan *P, unsigned long batch, const IoShape &io, mpfr_t *inr, mpfr_t *ini,
                         uint32_t *planes, long *exps) {
-  const unsigned long N = P->N;
+  const unsigned long N = io.n;
   const int L = P->L;
   // block exponents and finiteness
   std::vector<int> bad(batch, 0);
@@ -445,7 +466,7 @@ static int mp_pack_impl(const mpfft_mp_plan *P, unsigned long batch, mpfr_t *inr
       long e_s = LONG_MIN;
       for (unsigned long p = 0; p < N; ++p) {
         for (int c = 0; c < 2; ++c) {
-          mpfr_srcptr x = elem(c ? ini : inr, b, N, p, s);
+          mpfr_srcptr x = elem(c ? ini : inr, b, io, p);
           if (!mpfr_number_p(x)) bad[b] = 1;
           else if (!mpfr_zero_p(x) && x->_mpfr_exp > e_s) e_s = x->_mpfr_exp;
         }
@@ -461,7 +482,7 @@ static int mp_pack_impl(const mpfft_mp_plan *P, unsigned long batch, mpfr_t *inr
     for (long t = a0; t < a1; ++t) {
       const unsigned long p = t / batch, b = t % batch;
       for (int c = 0; c < 2; ++c) {
-        uint32_t sg = mpfr_to_fixed(elem(c ? ini : inr, b, N, p, s), L, P->F, exps[b], tmp);
+        uint32_t sg = mpfr_to_fixed(elem(c ? ini : inr, b, io, p), L, P->F, exps[b], tmp);
         if (sg) {  // two's complement
           uint32_t cy = 1;
           for (int i = 0; i < L; ++i) {
@@ -478,12 +499,12 @@ static int mp_pack_impl(const mpfft_mp_plan *P, unsigned long batch, mpfr_t *inr
   return MPFFT_OK;
 }
 
+// fadj: the value of fixed-point integer A is A * 2^(exps[b] - F - fadj)
 static void mp_unpack_impl(const mpfft_mp_plan *P, unsigned long batch, const uint32_t *planes, const long *exps,
-                           mpfr_t *outr, mpfr_t *outi, unsigned flags) {
-  const unsigned long N = P->N;
+                           const IoShape &io, mpfr_t *outr, mpfr_t *outi, long fadj) {
+  const unsigned long N = io.n;
   const int L = P->L;
   const size_t plane = (size_t)N * batch;
-  const long shift = (flags & MPFFT_SCALED) ? ilog2(N) : 0;
   parallel_for((long)(N * batch), 256, [&](long a0, long a1) {
     uint32_t tmp[kMaxLimbsBig + 2];
     for (long t = a0; t < a1; ++t) {
@@ -491,7 +512,7 @@ static void mp_unpack_impl(const mpfft_mp_plan *P, unsigned long batch, const ui
       for (int c = 0; c < 2; ++c) {
         const uint32_t *src = planes + (size_t)c * L * plane + (size_t)p * batch + b;
         for (int i = 0; i < L; ++i) tmp[i] = src[(size_t)i * plane];
-        fixed_to_mpfr(tmp, L, exps[b] - P->F - shift, (c ? outi : outr)[b * N + p]);
+        fixed_to_mpfr(tmp, L, exps[b] - P->F - fadj, elem(c ? outi : outr, b, io, p));
       }
     }
   });
@@ -505,8 +526,8 @@ static void mp_fill_nan(mpfr_t *a, unsigned long n) {
 static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int nlo) {
   if (chunk <= p->cv_chunk && nli <= p->cv_nli && nlo <= p->cv_nlo) return MPFFT_OK;
   p->free_conv();
-  const size_t comp = (size_t)2 * p->N * chunk;
-  const size_t words = (size_t)2 * p->L * p->N * chunk;
+  const size_t comp = (size_t)2 * p->pts_max() * chunk;
+  const size_t words = (size_t)2 * p->L * p->pts_max() * chunk;
   bool ok = true;
   auto dm = [&](void **q, size_t bytes) { ok = ok && cudaMalloc(q, bytes) == cudaSuccess; };
   auto hm = [&](void **q, size_t bytes) { ok = ok && cudaMallocHost(q, bytes) == cudaSuccess; };
@@ -543,76 +564,98 @@ static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int n
 
 static inline int nlimbs64(long prec) { return (int)((prec + 63) / 64); }
 
+// Device work between import and export.  a holds the imported input; the
+// result ends in *res (a or b).  complex: transform a -> b.  R2C: transform
+// a -> b, split b -> a (half spectrum, value 2X).  C2R: split a -> b (2Z with
+// planes exchanged), transform b -> a (planes exchanged: the inverse).
+static cudaError_t mp_device_pipeline(const mpfft_mp_plan *p, int mode, uint32_t *a, uint32_t *b, int B,
+                                      cudaStream_t st, uint32_t *big, uint32_t **res) {
+  cudaError_t e = cudaSuccess;
+  if (mode == kComplex) {
+    *res = b;
+    return mp_run_transform(p->L, p->tabs, a, b, B, st, nullptr, big);
+  }
+  *res = a;
+  if (mode == kR2C) {
+    if ((e = mp_run_transform(p->L, p->tabs, a, b, B, st, nullptr, big)) != cudaSuccess) return e;
+    return mp_real_split(true, p->L, b, a, (int)p->N, B, p->tabs.tw, p->tabs.dneg, st);
+  }
+  if ((e = mp_real_split(false, p->L, a, b, (int)p->N, B, p->tabs.tw, p->tabs.dneg, st)) != cudaSuccess) return e;
+  return mp_run_transform(p->L, p->tabs, b, a, B, st, nullptr, big);
+}
+
 // All inputs with one limb count and all outputs with one precision: the
 // conversion runs on the GPU and the host only moves raw significand limbs.
 // The batch is processed in chunks through two slots (stream + staging each):
 // while the GPU copies and transforms chunk i, the host scatters chunk i-1's
 // results and gathers chunk i+1's inputs.  Returns -1 when the call does not
-// qualify (mixed precisions).
-static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr, mpfr_t *ini, unsigned long s,
-                              mpfr_t *outr, mpfr_t *outi, unsigned flags) {
-  const unsigned long N = p->N;
+// qualify (mixed precisions).  fadj: output value = A * 2^(e_s - F - fadj).
+static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, const IoShape &ii, mpfr_t *inr,
+                              mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj) {
+  const unsigned long Ni = ii.n, No = oo.n;
   const long prec_out = mpfr_get_prec(outr[0]);
   const int nli = nlimbs64(mpfr_get_prec(inr[0])), nlo = nlimbs64(prec_out);
   std::vector<int> bad(batch, 0);
   parallel_for((long)batch, 1, [&](long b0, long b1) {
-    for (long b = b0; b < b1; ++b)
-      for (unsigned long q = 0; q < N && !bad[b]; ++q) {
-        mpfr_srcptr a = elem(inr, b, N, q, s), c = elem(ini, b, N, q, s);
+    for (long b = b0; b < b1; ++b) {
+      for (unsigned long q = 0; q < Ni && !bad[b]; ++q) {
+        mpfr_srcptr a = elem(inr, b, ii, q), c = elem(ini, b, ii, q);
         if (nlimbs64(a->_mpfr_prec) != nli || nlimbs64(c->_mpfr_prec) != nli) bad[b] = 1;
-        else if (outr[b * N + q]->_mpfr_prec != prec_out || outi[b * N + q]->_mpfr_prec != prec_out) bad[b] = 1;
       }
+      for (unsigned long q = 0; q < No && !bad[b]; ++q)
+        if (elem(outr, b, oo, q)->_mpfr_prec != prec_out || elem(outi, b, oo, q)->_mpfr_prec != prec_out) bad[b] = 1;
+    }
   });
   for (unsigned long b = 0; b < batch; ++b)
     if (bad[b]) return -1;
   // chunks of up to 256 signals (a multiple of 32 keeps every warp on one
   // butterfly), and at most ~256 MiB of staging per slot
-  const size_t per_signal = (size_t)2 * N * ((nli + nlo) * 8 + 2 * 4 * p->L + 18);
+  const size_t per_signal = (size_t)2 * p->pts_max() * ((nli + nlo) * 8 + 2 * 4 * p->L + 18);
   unsigned long chunk = std::min<unsigned long>(256, std::max<size_t>(32, (256UL << 20) / per_signal));
   if (chunk >= 32) chunk &= ~31UL;
   chunk = std::min(chunk, batch);
   if (int e = mp_conv_reserve(p, chunk, nli, nlo)) return e;
   const unsigned long nchunks = (batch + chunk - 1) / chunk;
-  const long shift = (flags & MPFFT_SCALED) ? ilog2(N) : 0;
   const long emin = mpfr_get_emin(), emax = mpfr_get_emax();
   std::vector<int> nonfin(nchunks, 0);
 
   auto gather = [&](unsigned long ci) {
     auto &c = p->cv[ci & 1];
     const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
-    parallel_for((long)(2 * cb * N), 2048, [&](long x0, long x1) {
+    parallel_for((long)(2 * cb * Ni), 2048, [&](long x0, long x1) {
       for (long u = x0; u < x1; ++u) {
-            const long bb = u / (2 * (long)N), part = (u / (long)N) & 1;
-            const unsigned long q = (unsigned long)(u % (long)N);
-            mpfr_srcptr x = elem(part ? ini : inr, b0 + bb, N, q, s);
-            const size_t t = ((size_t)part * N + q) * cb + bb;
-            if (x->_mpfr_exp <= LONG_MIN + 3) {  // MPFR's reserved exponents: zero, NaN, infinity
-              if (!mpfr_zero_p(x)) nonfin[ci] = 1;
-              c.h_ei[t] = INT64_MIN;
-              c.h_si[t] = 0;
-              memset(c.h_mi + t * nli, 0, nli * 8);
-            } else {
-              c.h_ei[t] = x->_mpfr_exp;
-              c.h_si[t] = x->_mpfr_sign < 0;
-              memcpy(c.h_mi + t * nli, x->_mpfr_d, nli * 8);
-            }
-          }
+        const long bb = u / (2 * (long)Ni), part = (u / (long)Ni) & 1;
+        const unsigned long q = (unsigned long)(u % (long)Ni);
+        mpfr_srcptr x = elem(part ? ini : inr, b0 + bb, ii, q);
+        const size_t t = ((size_t)part * Ni + q) * cb + bb;
+        if (x->_mpfr_exp <= LONG_MIN + 3) {  // MPFR's reserved exponents: zero, NaN, infinity
+          if (!mpfr_zero_p(x)) nonfin[ci] = 1;
+          c.h_ei[t] = INT64_MIN;
+          c.h_si[t] = 0;
+          memset(c.h_mi + t * nli, 0, nli * 8);
+        } else {
+          c.h_ei[t] = x->_mpfr_exp;
+          c.h_si[t] = x->_mpfr_sign < 0;
+          memcpy(c.h_mi + t * nli, x->_mpfr_d, nli * 8);
+        }
+      }
     });
   };
   auto launch = [&](unsigned long ci) -> int {
     auto &c = p->cv[ci & 1];
     const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
-    const size_t comp = (size_t)2 * N * cb;
-    CUDA_TRY(cudaMemcpyAsync(c.d_mi, c.h_mi, comp * nli * 8, cudaMemcpyHostToDevice, c.st));
-    CUDA_TRY(cudaMemcpyAsync(c.d_ei, c.h_ei, comp * 8, cudaMemcpyHostToDevice, c.st));
-    CUDA_TRY(cudaMemcpyAsync(c.d_si, c.h_si, comp, cudaMemcpyHostToDevice, c.st));
-    CUDA_TRY(mp_import_launch(c.d_mi, c.d_ei, c.d_si, nli, (int)N, (int)cb, p->L, p->F, c.d_es, c.d_in, c.st));
-    CUDA_TRY(mp_run_transform(p->L, p->tabs, c.d_in, c.d_out, (int)cb, c.st, nullptr, c.d_big));
-    CUDA_TRY(mp_export_launch(c.d_out, (int)N, (int)cb, p->L, c.d_es, p->F + shift, prec_out, nlo, c.d_mo, c.d_eo,
+    const size_t ci_n = (size_t)2 * Ni * cb, co_n = (size_t)2 * No * cb;
+    CUDA_TRY(cudaMemcpyAsync(c.d_mi, c.h_mi, ci_n * nli * 8, cudaMemcpyHostToDevice, c.st));
+    CUDA_TRY(cudaMemcpyAsync(c.d_ei, c.h_ei, ci_n * 8, cudaMemcpyHostToDevice, c.st));
+    CUDA_TRY(cudaMemcpyAsync(c.d_si, c.h_si, ci_n, cudaMemcpyHostToDevice, c.st));
+    CUDA_TRY(mp_import_launch(c.d_mi, c.d_ei, c.d_si, nli, (int)Ni, (int)cb, p->L, p->F, c.d_es, c.d_in, c.st));
+    uint32_t *res = nullptr;
+    CUDA_TRY(mp_device_pipeline(p, mode, c.d_in, c.d_out, (int)cb, c.st, c.d_big, &res));
+    CUDA_TRY(mp_export_launch(res, (int)No, (int)cb, p->L, c.d_es, p->F + fadj, prec_out, nlo, c.d_mo, c.d_eo,
                               c.d_so, c.st));
-    CUDA_TRY(cudaMemcpyAsync(c.h_mo, c.d_mo, comp * nlo * 8, cudaMemcpyDeviceToHost, c.st));
-    CUDA_TRY(cudaMemcpyAsync(c.h_eo, c.d_eo, comp * 8, cudaMemcpyDeviceToHost, c.st));
-    CUDA_TRY(cudaMemcpyAsync(c.h_so, c.d_so, comp, cudaMemcpyDeviceToHost, c.st));
+    CUDA_TRY(cudaMemcpyAsync(c.h_mo, c.d_mo, co_n * nlo * 8, cudaMemcpyDeviceToHost, c.st));
+    CUDA_TRY(cudaMemcpyAsync(c.h_eo, c.d_eo, co_n * 8, cudaMemcpyDeviceToHost, c.st));
+    CUDA_TRY(cudaMemcpyAsync(c.h_so, c.d_so, co_n, cudaMemcpyDeviceToHost, c.st));
     CUDA_TRY(cudaEventRecord(c.done, c.st));
     return MPFFT_OK;
   };
@@ -620,27 +663,27 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr
     auto &c = p->cv[ci & 1];
     CUDA_TRY(cudaEventSynchronize(c.done));
     const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
-    parallel_for((long)(2 * cb * N), 2048, [&](long x0, long x1) {
+    parallel_for((long)(2 * cb * No), 2048, [&](long x0, long x1) {
       for (long u = x0; u < x1; ++u) {
-            const long bb = u / (2 * (long)N), part = (u / (long)N) & 1;
-            const unsigned long q = (unsigned long)(u % (long)N);
-            mpfr_ptr y = (part ? outi : outr)[(b0 + bb) * N + q];
-            const size_t t = ((size_t)part * N + q) * cb + bb;
-            const int64_t e = c.h_eo[t];
-            if (e == INT64_MIN) {
-              mpfr_set_zero(y, 1);
-            } else if (e >= emin && e <= emax) {
-              memcpy(y->_mpfr_d, c.h_mo + t * nlo, nlo * 8);
-              y->_mpfr_exp = e;
-              y->_mpfr_sign = c.h_so[t] ? -1 : 1;
-            } else {  // outside the current exponent range: let MPFR overflow/underflow
-              __mpz_struct z;
-              z._mp_alloc = nlo;
-              z._mp_size = c.h_so[t] ? -nlo : nlo;
-              z._mp_d = reinterpret_cast<mp_limb_t *>(c.h_mo + t * nlo);
-              mpfr_set_z_2exp(y, &z, e - 64L * nlo, MPFR_RNDN);
-            }
-          }
+        const long bb = u / (2 * (long)No), part = (u / (long)No) & 1;
+        const unsigned long q = (unsigned long)(u % (long)No);
+        mpfr_ptr y = elem(part ? outi : outr, b0 + bb, oo, q);
+        const size_t t = ((size_t)part * No + q) * cb + bb;
+        const int64_t e = c.h_eo[t];
+        if (e == INT64_MIN) {
+          mpfr_set_zero(y, 1);
+        } else if (e >= emin && e <= emax) {
+          memcpy(y->_mpfr_d, c.h_mo + t * nlo, nlo * 8);
+          y->_mpfr_exp = e;
+          y->_mpfr_sign = c.h_so[t] ? -1 : 1;
+        } else {  // outside the current exponent range: let MPFR overflow/underflow
+          __mpz_struct z;
+          z._mp_alloc = nlo;
+          z._mp_size = c.h_so[t] ? -nlo : nlo;
+          z._mp_d = reinterpret_cast<mp_limb_t *>(c.h_mo + t * nlo);
+          mpfr_set_z_2exp(y, &z, e - 64L * nlo, MPFR_RNDN);
+        }
+      }
     });
     return MPFFT_OK;
   };
@@ -684,26 +727,34 @@ static int mp_big_reserve(mpfft_mp_plan *p, unsigned long batch, uint32_t **out)
   return MPFFT_OK;
 }
 
-static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr, mpfr_t *ini, unsigned long s,
-                           mpfr_t *outr, mpfr_t *outi, unsigned flags) {
+static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, int mode, const IoShape &ii, mpfr_t *inr,
+                           mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj) {
   if (p->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
   std::lock_guard<std::mutex> g(p->mu);
   if (!p->force_host_conversion) {
-    const int r = mp_execute_gpuconv(p, batch, inr, ini, s, outr, outi, flags);
+    const int r = mp_execute_gpuconv(p, batch, mode, ii, inr, ini, oo, outr, outi, fadj);
     if (r != -1) return r;
   }
   if (int e = mp_reserve(p, batch)) return e;
   p->exps.assign(batch, 0);
-  if (int e = mp_pack_impl(p, batch, inr, ini, s, p->h_in, p->exps.data())) return e;
-  const size_t bytes = (size_t)2 * p->L * p->N * batch * 4;
+  if (int e = mp_pack_impl(p, batch, ii, inr, ini, p->h_in, p->exps.data())) return e;
   uint32_t *big = nullptr;
   if (int e = mp_big_reserve(p, batch, &big)) return e;
-  CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, bytes, cudaMemcpyHostToDevice, p->stream));
-  CUDA_TRY(mp_run_transform(p->L, p->tabs, p->d_in, p->d_out, (int)batch, p->stream, nullptr, big));
-  CUDA_TRY(cudaMemcpyAsync(p->h_out, p->d_out, bytes, cudaMemcpyDeviceToHost, p->stream));
+  uint32_t *res = nullptr;
+  CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, (size_t)2 * p->L * ii.n * batch * 4, cudaMemcpyHostToDevice,
+                           p->stream));
+  CUDA_TRY(mp_device_pipeline(p, mode, p->d_in, p->d_out, (int)batch, p->stream, big, &res));
+  CUDA_TRY(cudaMemcpyAsync(p->h_out, res, (size_t)2 * p->L * oo.n * batch * 4, cudaMemcpyDeviceToHost, p->stream));
   CUDA_TRY(cudaStreamSynchronize(p->stream));
-  mp_unpack_impl(p, batch, p->h_out, p->exps.data(), outr, outi, flags);
+  mp_unpack_impl(p, batch, p->h_out, p->exps.data(), oo, outr, outi, fadj);
   return set_err(MPFFT_OK, "");
+}
+
+// complex transform of strided host arrays (input stride s, contiguous output)
+static int mp_execute_complex(mpfft_mp_plan *p, unsigned long batch, mpfr_t *inr, mpfr_t *ini, unsigned long s,
+                              mpfr_t *outr, mpfr_t *outi, unsigned flags) {
+  const long shift = (flags & MPFFT_SCALED) ? ilog2(p->N) : 0;
+  return mp_execute_impl(p, batch, kComplex, io_signals(p->N, s), inr, ini, io_signals(p->N, 1), outr, outi, shift);
 }
 
 static long mp_call_prec(mpfr_t *inr, mpfr_t *ini, mpfr_t *outr, mpfr_t *outi) {
@@ -733,7 +784,7 @@ static void mp_dropin(unsigned long n, unsigned long s, long sn, mpfr_t *inr, mp
   if (e == MPFFT_OK) {
     mpfft_mp_plan *p = mp_cached(n, mp_call_prec(inr, ini, outr, outi));
     if (!p) e = g_err;
-    else e = mp_execute_impl(p, 1, inr, ini, s, outr, outi, flags);
+    else e = mp_execute_complex(p, 1, inr, ini, s, outr, outi, flags);
   }
   if (e != MPFFT_OK) {
     mp_fill_nan(outr, n);
@@ -1011,7 +1062,8 @@ MPFFT_API int mpfft_mp_execute(mpfft_mp_plan *plan, unsigned long batch, mpfr_t 
     std::swap(outr, outi);
     flags &= ~MPFFT_INVERSE;
   }
-  int e = mp_execute_impl(plan, batch, inr, ini, 1, outr, outi, flags);
+  if (plan->real) return set_err(MPFFT_EINVAL, "real plan: use mpfft_mp_execute_r2c / mpfft_mp_execute_c2r");
+  int e = mp_execute_complex(plan, batch, inr, ini, 1, outr, outi, flags);
   if (e != MPFFT_OK) {
     mp_fill_nan(outr, plan->N * batch);
     mp_fill_nan(outi, plan->N * batch);
@@ -1019,10 +1071,55 @@ MPFFT_API int mpfft_mp_execute(mpfft_mp_plan *plan, unsigned long batch, mpfr_t 
   return e;
 }
 
+MPFFT_API int mpfft_mp_plan_create_real(mpfft_mp_plan **plan, unsigned long n, long prec, unsigned flags) {
+  if (!plan) return set_err(MPFFT_EINVAL, "NULL plan pointer");
+  *plan = nullptr;
+  if (flags & MPFFT_PLAN_HOST_ONLY) return set_err(MPFFT_EINVAL, "real plans have no host-only form");
+  std::unique_ptr<mpfft_mp_plan> p(new (std::nothrow) mpfft_mp_plan);
+  if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
+  if (int e = mp_plan_init(p.get(), n, prec, false, true)) return e;
+  p->force_host_conversion = (flags & MPFFT_PLAN_HOST_CONVERSION) != 0;
+  *plan = p.release();
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_mp_execute_r2c(mpfft_mp_plan *plan, unsigned long batch, mpfr_t *in, mpfr_t *outr,
+                                   mpfr_t *outi, unsigned flags) {
+  if (!plan || !in || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (!plan->real) return set_err(MPFFT_EINVAL, "not a real plan (mpfft_mp_plan_create_real)");
+  if (flags & MPFFT_INVERSE) return set_err(MPFFT_EINVAL, "MPFFT_INVERSE: use mpfft_mp_execute_c2r");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  const unsigned long n = plan->n_real, m = plan->N;
+  // x_(2j) -> real plane, x_(2j+1) -> imaginary plane of the m-point complex signal
+  const IoShape ii{m, n, 2}, oo{m + 1, m + 1, 1};
+  const long fadj = 1 + ((flags & MPFFT_SCALED) ? ilog2(n) : 0);  // the split step yields 2X
+  int e = mp_execute_impl(plan, batch, kR2C, ii, in, in + 1, oo, outr, outi, fadj);
+  if (e != MPFFT_OK) {
+    mp_fill_nan(outr, (m + 1) * batch);
+    mp_fill_nan(outi, (m + 1) * batch);
+  }
+  return e;
+}
+
+MPFFT_API int mpfft_mp_execute_c2r(mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr_t *ini,
+                                   mpfr_t *out, unsigned flags) {
+  if (!plan || !inr || !ini || !out) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (!plan->real) return set_err(MPFFT_EINVAL, "not a real plan (mpfft_mp_plan_create_real)");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  const unsigned long n = plan->n_real, m = plan->N;
+  // the result's real plane holds the odd samples, its imaginary plane the even ones
+  const IoShape ii{m + 1, m + 1, 1}, oo{m, n, 2};
+  const long fadj = (flags & MPFFT_SCALED) ? ilog2(n) : 0;
+  int e = mp_execute_impl(plan, batch, kC2R, ii, inr, ini, oo, out + 1, out, fadj);
+  if (e != MPFFT_OK) mp_fill_nan(out, n * batch);
+  return e;
+}
+
 MPFFT_API int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, const uint32_t *d_in,
                                       uint32_t *d_out, void *stream) {
   if (!plan || !d_in || !d_out) return set_err(MPFFT_EINVAL, "NULL argument");
   if (plan->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
+  if (plan->real) return set_err(MPFFT_EINVAL, "real plans have no device-layout entry point");
   if (batch == 0) return set_err(MPFFT_OK, "");
   const size_t bytes = (size_t)2 * plan->L * plan->N * batch * 4;
   const char *a = (const char *)d_in, *b = (const char *)d_out;
@@ -1037,14 +1134,17 @@ MPFFT_API int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, 
 MPFFT_API int mpfft_mp_pack(const mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr_t *ini,
                             uint32_t *planes, long *exps) {
   if (!plan || !inr || !ini || !planes || !exps) return set_err(MPFFT_EINVAL, "NULL argument");
-  if (int e = mp_pack_impl(plan, batch, inr, ini, 1, planes, exps)) return e;
+  if (plan->real) return set_err(MPFFT_EINVAL, "pack/unpack take complex plans");
+  if (int e = mp_pack_impl(plan, batch, io_signals(plan->N, 1), inr, ini, planes, exps)) return e;
   return set_err(MPFFT_OK, "");
 }
 
 MPFFT_API int mpfft_mp_unpack(const mpfft_mp_plan *plan, unsigned long batch, const uint32_t *planes,
                               const long *exps, mpfr_t *outr, mpfr_t *outi, unsigned flags) {
   if (!plan || !outr || !outi || !planes || !exps) return set_err(MPFFT_EINVAL, "NULL argument");
-  mp_unpack_impl(plan, batch, planes, exps, outr, outi, flags);
+  if (plan->real) return set_err(MPFFT_EINVAL, "pack/unpack take complex plans");
+  mp_unpack_impl(plan, batch, planes, exps, io_signals(plan->N, 1), outr, outi,
+                 (flags & MPFFT_SCALED) ? ilog2(plan->N) : 0);
   return set_err(MPFFT_OK, "");
 }
 
@@ -1104,6 +1204,7 @@ MPFFT_API int mpfft_mp_execute_device_timed(mpfft_mp_plan *plan, unsigned long b
                                             uint32_t *d_out, void *stream, float *launch_ms) {
   if (!plan || !d_in || !d_out || !launch_ms) return set_err(MPFFT_EINVAL, "NULL argument");
   if (plan->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
+  if (plan->real) return set_err(MPFFT_EINVAL, "real plans have no device-layout entry point");
   uint32_t *big = nullptr;
   if (int e = mp_big_reserve(plan, batch, &big)) return e;
   CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream, launch_ms, big));
@@ -1129,6 +1230,7 @@ MPFFT_API int mpfft_mp_execute_significands_static(const mpfft_mp_plan *plan, un
   if (!plan || !d_mant_in || !d_exp_in || !d_sign_in || !d_mant_out || !d_exp_out || !d_sign_out)
     return set_err(MPFFT_EINVAL, "NULL argument");
   if (plan->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
+  if (plan->real) return set_err(MPFFT_EINVAL, "real plans have no device-layout entry point");
   if (nl_in < 1 || prec_out < 2) return set_err(MPFFT_EINVAL, "nl_in must be >= 1 and prec_out >= 2");
   if (batch == 0) return set_err(MPFFT_OK, "");
   if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");

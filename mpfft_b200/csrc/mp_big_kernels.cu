@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(256) mp_big_leaf_kernel(const uint32_t *__rest
 __global__ void __launch_bounds__(128) mp_big_level_kernel(uint32_t *__restrict__ y, int N, int B, int L, int n,
                                                             const int *__restrict__ node_off, int nnodes,
                                                             const uint32_t *__restrict__ tw,
-                                                            const uint8_t *__restrict__ dneg,
+                                                            const uint8_t *__restrict__ dneg, int tws,
                                                             uint32_t *__restrict__ scratch) {
   const int q = n >> 2;
   const long long total = (long long)nnodes * q * B;
@@ -226,8 +226,8 @@ __global__ void __launch_bounds__(128) mp_big_level_kernel(uint32_t *__restrict_
   const size_t ss = (size_t)total;                   // scratch limb-plane stride
   uint32_t *AX = scratch + t;                        // |operand|
   uint32_t *P = scratch + (size_t)L * ss + t;        // first product of the side
-  const size_t tplane = (size_t)(N >> 2);
-  const int kn = k * (N / n);
+  const size_t tplane = (size_t)(N >> 2) * tws;
+  const int kn = k * (N / n) * tws;
   const uint32_t *wr = tw + kn, *ws = tw + (size_t)L * tplane + kn, *wd = tw + (size_t)2 * L * tplane + kn;
   const bool special = 2 * k == q;
   const bool dn = special ? false : (dneg[kn] != 0);
@@ -303,7 +303,7 @@ cudaError_t mp_big_run_transform(int L, const MpDeviceTables &T, const uint32_t 
     const long long total = (long long)T.level_count[lv] * (n / 4) * B;
     timer.begin();
     mp_big_level_kernel<<<(int)((total + 127) / 128), 128, 0, s>>>(out, T.N, B, L, n, T.node_off + T.level_start[lv],
-                                                                   T.level_count[lv], T.tw, T.dneg, scratch);
+                                                                   T.level_count[lv], T.tw, T.dneg, T.tws, scratch);
     timer.end();
   }
   return cudaGetLastError();

@@ -158,7 +158,7 @@ template <int L>
 __global__ void __launch_bounds__(128, 4) mp_level_kernel(uint32_t *__restrict__ y, int N, int B, int n,
                                                           const int *__restrict__ node_off, int nnodes,
                                                           const uint32_t *__restrict__ tw,
-                                                          const uint8_t *__restrict__ dneg) {
+                                                          const uint8_t *__restrict__ dneg, int tws) {
   __shared__ uint32_t Ps[L * 128];
   const int q = n >> 2;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -178,8 +178,8 @@ __global__ void __launch_bounds__(128, 4) mp_level_kernel(uint32_t *__restrict__
     combine<L>(u0, u1, zp, zm, plane, cim, false);
     return;
   }
-  const size_t tplane = (size_t)(N >> 2);  // twiddle limb-plane stride
-  const int kn = k * (N / n);
+  const size_t tplane = (size_t)(N >> 2) * tws;  // twiddle limb-plane stride
+  const int kn = k * (N / n) * tws;
   const uint32_t *wr = tw + kn;                           // cos
   const uint32_t *ws = tw + (size_t)L * tplane + kn;      // cos + sin
   const uint32_t *wd = tw + (size_t)2 * L * tplane + kn;  // |cos - sin|
@@ -266,7 +266,7 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
     const int blocks = (int)((total + lthreads - 1) / lthreads);
     timer.begin();
     mp_level_kernel<L><<<blocks, lthreads, 0, s>>>(out, T.N, B, n, T.node_off + T.level_start[lv],
-                                                   T.level_count[lv], T.tw, T.dneg);
+                                                   T.level_count[lv], T.tw, T.dneg, T.tws);
     timer.end();
   }
   return cudaGetLastError();

@@ -37,8 +37,9 @@ struct TreeTables {
 };
 
 struct MpDeviceTables : TreeTables {
-  const uint32_t *tw = nullptr;   // [3][L][N/4]: cos, cos+sin, |cos-sin| magnitudes
-  const uint8_t *dneg = nullptr;  // [N/4]: sign of cos-sin
+  const uint32_t *tw = nullptr;   // [3][L][tws*N/4]: cos, cos+sin, |cos-sin| magnitudes
+  const uint8_t *dneg = nullptr;  // [tws*N/4]: sign of cos-sin
+  int tws = 1;  // the table is built for tws*N points (2 for a real transform of 2N points)
 };
 
 // Schedule of one shared-memory sub-transform of size `size` (FP64 tier):
@@ -134,6 +135,11 @@ size_t mp_big_scratch_words(const MpDeviceTables &T, int L, int B);
 cudaError_t mp_big_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
                                  uint32_t *scratch, cudaStream_t s, float *launch_ms);
 cudaError_t diag_imad_rate(int wide, double *ops_per_s);
+// Split step of a real transform of 2M points (L <= kMaxLimbs; tw/dneg: the
+// table of a 2M-point plan).  forward: Z (M points) -> 2X (M+1 points);
+// otherwise half spectrum X (M+1 points) -> 2Z with its planes exchanged.
+cudaError_t mp_real_split(bool forward, int L, const uint32_t *in, uint32_t *out, int M, int B, const uint32_t *tw,
+                          const uint8_t *dneg, cudaStream_t s);
 
 // GPU-side conversion between MPFR significands and limb planes.  Component
 // (c, p, b) is index (c*N + p)*B + b of the mant/ex/sg arrays; ex = INT64_MIN

@@ -84,6 +84,24 @@ OAPI void orc_mp_scale2(mpfr_t *a, unsigned long n, long e) {
   for (unsigned long k = 0; k < n; k++) mpfr_mul_2si(a[k], a[k], e, RN);
 }
 
+/* Full spectrum of a real signal of n >= 2 points from its half spectrum
+ * h[0..n/2]: f[k] = h[k] for k <= n/2 and f[n-k] = conj h[k] for 0 < k < n/2;
+ * the imaginary parts of f[0] and f[n/2] are set to zero (a real signal's
+ * spectrum has none there).  Used to state the inverse real transform as a
+ * complex DFT. */
+OAPI void orc_mp_hermitian_extend(unsigned long n, mpfr_t *hr, mpfr_t *hi, mpfr_t *fr, mpfr_t *fi) {
+  const unsigned long m = n / 2;
+  for (unsigned long k = 0; k <= m; k++) {
+    mpfr_set(fr[k], hr[k], RN);
+    if (k == 0 || k == m) mpfr_set_ui(fi[k], 0, RN);
+    else mpfr_set(fi[k], hi[k], RN);
+  }
+  for (unsigned long k = 1; k < m; k++) {
+    mpfr_set(fr[n - k], hr[k], RN);
+    mpfr_neg(fi[n - k], hi[k], RN);
+  }
+}
+
 OAPI void orc_mp_set_nan(mpfr_t *a, unsigned long k) { mpfr_set_nan(a[k]); }
 OAPI void orc_mp_set_inf(mpfr_t *a, unsigned long k, int sign) { mpfr_set_inf(a[k], sign); }
 

@@ -68,6 +68,7 @@ def lib() -> C.CDLL:
         "orc_mp_fft": (None, [vp, ul, ul, sl, vp, vp, vp, vp]),
         "orc_mp_fft_top": (None, [vp, vp, vp, vp, vp]),
         "orc_mp_dft": (None, [ul, sl, vp, vp, vp, vp]),
+        "orc_mp_hermitian_extend": (None, [ul, vp, vp, vp, vp]),
         "orc_mp_errors": (None, [ul, vp, vp, vp, vp, dp]),
         "orc_d_new": (vp, [ul]),
         "orc_d_delete": (None, [vp]),

@@ -136,3 +136,15 @@ def test_no_gpu_fails_loudly(M, orc):
     assert M.d_sr24_cp_fft(16, 1, 0, d, d, o, o) == M.ECUDA
     with pytest.raises(M.MpfftError):
         M.MpPlan(16, 64)
+
+
+def test_real_plan_argument_validation(M):
+    """Real plans: n must be a power of two >= 2 and the format must fit the
+    register kernels (checked before any device work, so no GPU is needed)."""
+    for n in (0, 1, 3, 12):
+        with pytest.raises(M.MpfftError) as e:
+            M.MpRealPlan(n, 64)
+        assert e.value.code == M.EINVAL
+    with pytest.raises(M.MpfftError) as e:
+        M.MpRealPlan(1024, 2048)  # 66 limbs: beyond the 34-limb register kernels
+    assert e.value.code == M.EUNSUPPORTED
