@@ -54,6 +54,8 @@ extern "C" {
 #define MPFFT_INVERSE 8u        /* execute (host arrays): backward transform, exp(+2 pi i jk/n) */
 #define MPFFT_PLAN_HOST_ONLY 2u /* plan creation: conversion (pack/unpack) only, no device state */
 #define MPFFT_PLAN_HOST_CONVERSION 4u /* plan creation: convert mpfr_t <-> limbs on the host, not the GPU */
+#define MPFFT_PLAN_NO_TENSOR 16u /* plan creation: keep large-precision twiddle products on the integer
+                                     pipes (by default 64..260 limbs use int8 tensor-core GEMMs) */
 
 /* ------------------------------------------------------------------------ */
 /* 1. drop-in replacements for mpFFT.h                                      */
@@ -229,6 +231,17 @@ int mpfft_mp_execute_device_timed(mpfft_mp_plan *plan, unsigned long batch, cons
 /* Measured integer multiply-add rate of the current GPU (ops/s): wide = 0 for
  * 32-bit multiply-add, 1 for 32x32+64 -> 64-bit multiply-add. */
 int mpfft_diag_imad_rate(int wide, double *ops_per_s);
+/* The tensor-core twiddle product on its own: out = sign(x) * r for `batch`
+ * operands x (device limb planes x[i*batch + b], two's complement, L limbs,
+ * |x| < 2^(32L-2)) and one unsigned twiddle w[0..L-1], with
+ * r = floor((S + 2^(32L-2)) / 2^(32L-1)), S = the part of |x|*w in byte
+ * columns >= 4L-8 rounded down to a multiple of 16.  64 <= L <= 260.
+ * Asynchronous on `stream`. */
+int mpfft_diag_tc_mul(int limbs, unsigned long batch, const uint32_t *d_x, const uint32_t *d_w, uint32_t *d_out,
+                      void *stream);
+/* MPFFT_OK, or MPFFT_ECUDA if a bounded wait of a tensor-core kernel expired
+ * since the last call (the synchronous host-array calls check this themselves). */
+int mpfft_diag_tc_error(void);
 
 #ifdef __cplusplus
 }

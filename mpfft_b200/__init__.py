@@ -28,6 +28,7 @@ SCALED = 1
 PLAN_HOST_ONLY = 2
 PLAN_HOST_CONVERSION = 4
 INVERSE = 8
+PLAN_NO_TENSOR = 16
 
 
 class MpfftError(RuntimeError):
@@ -79,6 +80,8 @@ def _load() -> C.CDLL:
         "mpfft_mp_plan_schedule": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]),
         "mpfft_mp_execute_device_timed": (C.c_int, [vp, ul, u32p, u32p, vp, C.POINTER(C.c_float)]),
         "mpfft_diag_imad_rate": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+        "mpfft_diag_tc_mul": (C.c_int, [C.c_int, ul, vp, vp, vp, vp]),
+        "mpfft_diag_tc_error": (C.c_int, []),
         "mpfft_mp_execute_significands_static": (C.c_int, [vp, ul, vp, vp, vp, C.c_int, vp, vp, vp, sl, C.c_uint,
                                                            vp]),
         "mpfft_static_scratch_bytes": (C.c_size_t, []),
@@ -164,9 +167,11 @@ def d_sr24_cp_fft_scaled(n, s, sn, inr, ini, outr, outi) -> int:
 class MpPlan:
     """Multiprecision plan for n points at `prec` bits (device limb format)."""
 
-    def __init__(self, n: int, prec: int, host_only: bool = False, host_conversion: bool = False):
+    def __init__(self, n: int, prec: int, host_only: bool = False, host_conversion: bool = False,
+                 tensor: bool = True):
         h = C.c_void_p()
-        flags = (PLAN_HOST_ONLY if host_only else 0) | (PLAN_HOST_CONVERSION if host_conversion else 0)
+        flags = ((PLAN_HOST_ONLY if host_only else 0) | (PLAN_HOST_CONVERSION if host_conversion else 0)
+                 | (0 if tensor else PLAN_NO_TENSOR))
         _check(lib.mpfft_mp_plan_create_flags(C.byref(h), n, prec, flags))
         self.h = h
         self.n, self.prec = n, prec
@@ -242,6 +247,16 @@ class MpRealPlan:
 
     def c2r(self, batch, inr, ini, x, scaled=False) -> None:
         _check(lib.mpfft_mp_execute_c2r(self.h, batch, inr, ini, x, SCALED if scaled else 0))
+
+
+def tc_mul(limbs: int, batch: int, d_x: int, d_w: int, d_out: int, stream: int = 0) -> None:
+    """Tensor-core twiddle products of `batch` operands (device limb planes)."""
+    _check(lib.mpfft_diag_tc_mul(limbs, batch, d_x, d_w, d_out, stream or None))
+
+
+def tc_error() -> None:
+    """Raises if a bounded wait of a tensor-core kernel expired."""
+    _check(lib.mpfft_diag_tc_error())
 
 
 def imad_rate(wide: bool = False) -> float:

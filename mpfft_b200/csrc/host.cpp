@@ -727,13 +727,22 @@ static int mp_big_reserve(mpfft_mp_plan *p, unsigned long batch, uint32_t **out)
   return MPFFT_OK;
 }
 
+// after a synchronous execution: a tensor-core wait that expired voids the results
+static int mp_tc_check(const mpfft_mp_plan *p, int rc) {
+  if (rc != MPFFT_OK || !mp_tc_used(p->tabs, p->L)) return rc;
+  int code = 0;
+  CUDA_TRY(mp_tc_take_error(&code));
+  if (code) return set_err(MPFFT_ECUDA, "a tensor-core wait expired (code %d)", code);
+  return rc;
+}
+
 static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, int mode, const IoShape &ii, mpfr_t *inr,
                            mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj) {
   if (p->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
   std::lock_guard<std::mutex> g(p->mu);
   if (!p->force_host_conversion) {
     const int r = mp_execute_gpuconv(p, batch, mode, ii, inr, ini, oo, outr, outi, fadj);
-    if (r != -1) return r;
+    if (r != -1) return mp_tc_check(p, r);
   }
   if (int e = mp_reserve(p, batch)) return e;
   p->exps.assign(batch, 0);
@@ -746,6 +755,7 @@ static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, int mode, cons
   CUDA_TRY(mp_device_pipeline(p, mode, p->d_in, p->d_out, (int)batch, p->stream, big, &res));
   CUDA_TRY(cudaMemcpyAsync(p->h_out, res, (size_t)2 * p->L * oo.n * batch * 4, cudaMemcpyDeviceToHost, p->stream));
   CUDA_TRY(cudaStreamSynchronize(p->stream));
+  if (int e = mp_tc_check(p, MPFFT_OK)) return e;
   mp_unpack_impl(p, batch, p->h_out, p->exps.data(), oo, outr, outi, fadj);
   return set_err(MPFFT_OK, "");
 }
@@ -1037,6 +1047,7 @@ MPFFT_API int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, 
   if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
   if (int e = mp_plan_init(p.get(), n, prec, (flags & MPFFT_PLAN_HOST_ONLY) != 0)) return e;
   p->force_host_conversion = (flags & MPFFT_PLAN_HOST_CONVERSION) != 0;
+  if (flags & MPFFT_PLAN_NO_TENSOR) p->tabs.tc = 0;
   *plan = p.release();
   return set_err(MPFFT_OK, "");
 }
@@ -1209,6 +1220,24 @@ MPFFT_API int mpfft_mp_execute_device_timed(mpfft_mp_plan *plan, unsigned long b
   if (int e = mp_big_reserve(plan, batch, &big)) return e;
   CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream, launch_ms, big));
   return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_diag_tc_mul(int limbs, unsigned long batch, const uint32_t *d_x, const uint32_t *d_w,
+                                uint32_t *d_out, void *stream) {
+  if (!d_x || !d_w || !d_out) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (limbs < kTcMinLimbs || limbs > kTcMaxLimbs)
+    return set_err(MPFFT_EUNSUPPORTED, "limbs must be in [%d, %d]", kTcMinLimbs, kTcMaxLimbs);
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  if (int e = device_ready()) return e;
+  CUDA_TRY(mp_tc_mul(limbs, (int)batch, d_x, d_w, d_out, (cudaStream_t)stream));
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_diag_tc_error(void) {
+  int code = 0;
+  CUDA_TRY(mp_tc_take_error(&code));
+  return code ? set_err(MPFFT_ECUDA, "a tensor-core wait expired (code %d)", code) : set_err(MPFFT_OK, "");
 }
 
 MPFFT_API int mpfft_diag_imad_rate(int wide, double *ops_per_s) {

@@ -18,36 +18,12 @@
 // (error < L*2^-31 ulp) and the product is rounded to nearest.
 #include <cstdint>
 
+#include "mp_stream.cuh"
 #include "mpfft_internal.h"
 
 namespace mpfft {
 
 constexpr int kCB = 8;  // result columns per block
-
-__device__ __forceinline__ uint32_t add_c(uint32_t a, uint32_t b, uint32_t &c) {
-  const uint64_t t = (uint64_t)a + b + c;
-  c = (uint32_t)(t >> 32);
-  return (uint32_t)t;
-}
-
-// dst = pa +/- pb (or pa when pb is null), streamed; returns the sign bit of dst
-__device__ uint32_t big_addsub(uint32_t *dst, size_t ds, const uint32_t *pa, const uint32_t *pb, size_t ps, int L,
-                               bool sub) {
-  const uint32_t m = sub ? 0xffffffffu : 0u;
-  uint32_t c = sub ? 1u : 0u, v = 0;
-  for (int i = 0; i < L; ++i) {
-    v = pb ? add_c(pa[(size_t)i * ps], pb[(size_t)i * ps] ^ m, c) : pa[(size_t)i * ps];
-    dst[(size_t)i * ds] = v;
-  }
-  return v >> 31;
-}
-
-// x = -x in place when neg (two's complement)
-__device__ void big_cond_neg(uint32_t *x, size_t xs, int L, uint32_t neg) {
-  if (!neg) return;
-  uint32_t c = 1;
-  for (int i = 0; i < L; ++i) x[(size_t)i * xs] = add_c(~x[(size_t)i * xs], 0, c);
-}
 
 // Signed product streamed into its use:
 //   r = sign * round(|x| * w / 2^(32L-1))       (|x| in ax, sign = xneg)
@@ -121,29 +97,6 @@ __device__ void big_mul_merge(const uint32_t *ax, size_t as, const uint32_t *w, 
       }
       prev = limb;
     }
-  }
-}
-
-// The L-combine, streamed (see mp_kernels.cu combine()).
-__device__ void big_combine(uint32_t *u0, uint32_t *u1, uint32_t *zp, uint32_t *zm, size_t plane, size_t cim, int L,
-                            bool swapped) {
-  const size_t sre = swapped ? cim : 0, sim = swapped ? 0 : cim;
-  uint32_t ca1r = 0, ca1i = 0, ca2r = 1, ca2i = 1;
-  uint32_t c0r = 0, c2r = 1, c1r = 0, c3r = 1, c0i = 0, c2i = 1, c1i = 1, c3i = 0;
-  for (int i = 0; i < L; ++i) {
-    const size_t o = (size_t)i * plane;
-    const uint32_t U0r = u0[o], U0i = u0[o + cim], U1r = u1[o], U1i = u1[o + cim];
-    const uint32_t m1r = zp[o + sre], m1i = zp[o + sim], m2r = zm[o + sre], m2i = zm[o + sim];
-    const uint32_t a1r = add_c(m1r, m2r, ca1r), a1i = add_c(m1i, m2i, ca1i);
-    const uint32_t a2r = add_c(m1r, ~m2r, ca2r), a2i = add_c(m1i, ~m2i, ca2i);
-    u0[o] = add_c(U0r, a1r, c0r);
-    zp[o] = add_c(U0r, ~a1r, c2r);
-    u1[o] = add_c(U1r, a2i, c1r);
-    zm[o] = add_c(U1r, ~a2i, c3r);
-    u0[o + cim] = add_c(U0i, a1i, c0i);
-    zp[o + cim] = add_c(U0i, ~a1i, c2i);
-    u1[o + cim] = add_c(U1i, ~a2r, c1i);
-    zm[o + cim] = add_c(U1i, a2r, c3i);
   }
 }
 
@@ -286,7 +239,10 @@ size_t mp_big_scratch_words(const MpDeviceTables &T, int L, int B) {
     const long long th = (long long)T.level_count[lv] * (T.level_n[lv] / 4) * B;
     if (th > most) most = th;
   }
-  return (size_t)2 * L * (size_t)most;
+  const size_t words = (size_t)2 * L * (size_t)most;
+  if (!mp_tc_used(T, L)) return words;
+  const size_t tcw = mp_tc_scratch_words(T, L, B);
+  return tcw > words ? tcw : words;
 }
 
 cudaError_t mp_big_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
@@ -298,6 +254,7 @@ cudaError_t mp_big_run_transform(int L, const MpDeviceTables &T, const uint32_t 
     mp_big_leaf_kernel<<<(int)((total + 255) / 256), 256, 0, s>>>(in, out, T.N, B, L, T.leaves, T.nleaves);
     timer.end();
   }
+  if (mp_tc_used(T, L)) return mp_tc_run_levels(L, T, out, B, scratch, s, timer);
   for (int lv = 0; lv < T.nlevels; ++lv) {
     const int n = T.level_n[lv];
     const long long total = (long long)T.level_count[lv] * (n / 4) * B;

@@ -1,0 +1,521 @@
+// Multiprecision butterflies whose twiddle products run on the tensor cores
+// (tcgen05.mma kind::i8: unsigned 8-bit operands, exact int32 accumulation
+// in tensor memory), for large limb counts kTcMinLimbs <= L <= kTcMaxLimbs
+// (P from about 2000 to 8200 bits).
+//
+// Product as a matrix product.  At one level and one butterfly index k every
+// signal multiplies its operands by the same three twiddle constants (cos,
+// cos+sin, |cos-sin| of 2 pi k/N).  Write an operand |x| as 4L bytes x_a and a
+// twiddle w as 4L bytes w_c.  The byte columns of the product are
+//     D[m][j] = sum_a x_m[a] * w[j - a]      (each < 4L * 255^2 < 2^27)
+// i.e. the operand matrix X (signals m x bytes a) times a Toeplitz matrix of
+// twiddle bytes: a dense int8 GEMM with M = 128 signals per CTA, N = output
+// byte columns in tiles of 128, K = 4L operand bytes in steps of 32.
+//
+// The Toeplitz operand is never materialised.  In the no-swizzle K-major
+// shared-memory layout an MMA operand is made of core matrices of 8 rows x 16
+// bytes with a fixed 16-byte row stride; the descriptor gives the stride
+// between the two 16-byte K halves (LBO) and between 8-row groups (SBO).  Row
+// n = 8g + r of a tile is assigned output column j = J + g + 16(7 - r), and
+// group g reads copy g of the reversed twiddle bytes, shifted by g:
+//     copy_g[t] = w[Q + g - t],   B[n][a] = copy_g[Q - J - 112 + 16r + a]
+// so consecutive rows are 16 bytes apart (row r+1 is column j-16), the K
+// halves are 16 bytes apart (LBO = 16) and the groups are one copy apart
+// (SBO = copy length).  Sixteen copies of ~4L+320 bytes describe every
+// Toeplitz tile of every K step.
+//
+// Truncation and rounding.  Byte columns below J0 = 4L-8 (rounded down to a
+// multiple of 16) are not formed; the product is
+//     r = floor((sum_{j >= J0} D[j] 2^(8j) + 2^(32L-2)) / 2^(32L-1))
+// (the dropped part is below 4L * 2^-64 units of r's last place), with the
+// operand's sign applied afterwards.  The epilogue reads each signal's column
+// sums from its tensor-memory lane, carries them in increasing j and streams
+// the result limbs into their destination, merged with the first product of
+// the same side exactly as the streaming kernels do (mp_big_kernels.cu).
+//
+// Pipeline inside a CTA (128 threads, one per signal): operand bytes are
+// written to shared memory by all threads; thread 0 issues the MMAs of one
+// output tile into one of two 128-column tensor-memory buffers and commits
+// them to that buffer's mbarrier; while the epilogue drains tile t, the MMAs
+// of tile t+1 run.  Every wait is bounded (about two seconds of %globaltimer);
+// on expiry the kernel records an error code instead of hanging.
+#include <cstdint>
+
+#include "mp_stream.cuh"
+#include "mpfft_internal.h"
+
+namespace mpfft {
+
+constexpr int kTcRows = 128;                    // signals per CTA (MMA M)
+constexpr uint32_t kTcMinSmem = 80u * 1024u;    // at most two CTAs per SM: 2 x 256 TMEM columns
+constexpr uint32_t kTcTmemCols = 256;           // two 128-column accumulator buffers
+// instruction descriptor: D = s32, A = B = u8, both K-major, N = 128, M = 128
+constexpr uint32_t kTcIdesc = (2u << 4) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ int g_tc_error = 0;  // first error code of any CTA (0 = none)
+
+struct TcGeom {
+  int L, Kpad, J0, nt, Q, CL, wzw;
+  uint32_t offT, offWZ, offBar, offSlot, bytes;
+};
+
+__host__ __device__ inline TcGeom tc_geom(int L) {
+  TcGeom g;
+  g.L = L;
+  g.Kpad = (4 * L + 31) & ~31;            // operand bytes, padded to the MMA K step
+  g.J0 = (4 * L - 8) & ~15;               // first output byte column formed
+  g.nt = (8 * L - g.J0 + 127) / 128;      // output tiles of 128 columns
+  g.Q = (4 * L + 160 + 15) & ~15;         // reversal base of the twiddle copies
+  g.CL = (g.Q + 160 + 15) & ~15;          // bytes per copy (covers every tile and K step)
+  g.wzw = g.CL / 4 + 8;                   // words of a zero-padded twiddle
+  g.offT = 128u * g.Kpad;                 // operand rows first, then 3 x 16 copies
+  g.offWZ = g.offT + 48u * g.CL;
+  g.offBar = (g.offWZ + 12u * g.wzw + 15) & ~15u;
+  g.offSlot = g.offBar + 16;
+  g.bytes = g.offSlot + 16 > kTcMinSmem ? g.offSlot + 16 : kTcMinSmem;
+  return g;
+}
+
+// ---------------------------------------------------------------------------
+// PTX wrappers
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// shared-memory matrix descriptor: no swizzle, version 1 (sm_100)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// wait for the phase with the given parity to complete; false after ~2 s
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (global_ns() - t0 > 2000000000ull) return false;
+  }
+}
+
+#define MPFFT_TMEM_LD32(addr, v)                                                                                  \
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"  \
+               "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                        \
+               : "=r"((v)[0]), "=r"((v)[1]), "=r"((v)[2]), "=r"((v)[3]), "=r"((v)[4]), "=r"((v)[5]),             \
+                 "=r"((v)[6]), "=r"((v)[7]), "=r"((v)[8]), "=r"((v)[9]), "=r"((v)[10]), "=r"((v)[11]),           \
+                 "=r"((v)[12]), "=r"((v)[13]), "=r"((v)[14]), "=r"((v)[15]), "=r"((v)[16]), "=r"((v)[17]),       \
+                 "=r"((v)[18]), "=r"((v)[19]), "=r"((v)[20]), "=r"((v)[21]), "=r"((v)[22]), "=r"((v)[23]),       \
+                 "=r"((v)[24]), "=r"((v)[25]), "=r"((v)[26]), "=r"((v)[27]), "=r"((v)[28]), "=r"((v)[29]),       \
+                 "=r"((v)[30]), "=r"((v)[31])                                                                    \
+               : "r"(addr))
+
+// ---------------------------------------------------------------------------
+// CTA context: shared-memory layout, tensor memory, barriers
+// ---------------------------------------------------------------------------
+
+struct TcCtx {
+  TcGeom G;
+  uint8_t *smem;
+  uint32_t sA, sT, bar;  // shared addresses: operand rows, twiddle copies, 2 mbarriers
+  uint32_t tmem;         // tensor-memory base (lane 0, first column)
+  uint32_t ph;           // bit b: parity of the next completion of buffer b
+  int counter;           // output tiles processed so far (selects the buffer)
+  bool bad;              // a wait expired: stop waiting, results are void
+};
+
+// all threads; warp 0 allocates the tensor memory
+__device__ void tc_setup(TcCtx &c, uint8_t *smem, int L) {
+  c.G = tc_geom(L);
+  c.smem = smem;
+  c.sA = smem_addr(smem);
+  c.sT = c.sA + c.G.offT;
+  c.bar = c.sA + c.G.offBar;
+  c.ph = 0;
+  c.counter = 0;
+  c.bad = false;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(c.bar) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(c.bar + 8) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(c.sA + c.G.offSlot),
+                 "r"(kTcTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  c.tmem = *reinterpret_cast<volatile uint32_t *>(smem + c.G.offSlot);
+}
+
+__device__ void tc_teardown(TcCtx &c, int *err) {
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(c.tmem), "r"(kTcTmemCols) : "memory");
+  }
+  if (c.bad) atomicCAS(err, 0, 1);  // 1: a tensor-core wait expired
+}
+
+// Twiddle `which` (magnitude limbs w[l * tplane]) as 16 shifted reversed byte
+// copies: copy_g[t] = w_byte[Q + g - t] (zero outside 0 .. 4L-1).
+__device__ void tc_build_twiddle(TcCtx &c, int which, const uint32_t *w, size_t tplane) {
+  const TcGeom &G = c.G;
+  uint32_t *wz = reinterpret_cast<uint32_t *>(c.smem + G.offWZ) + which * G.wzw;
+  const int d4 = (G.CL - G.Q) / 4;  // wz byte u holds w_byte[u - (CL - Q)]
+  for (int u = threadIdx.x; u < G.wzw; u += blockDim.x) {
+    const int l = u - d4;
+    wz[u] = (l >= 0 && l < G.L) ? w[(size_t)l * tplane] : 0u;
+  }
+  __syncthreads();
+  uint32_t *T = reinterpret_cast<uint32_t *>(c.smem + G.offT + (size_t)which * 16 * G.CL);
+  const int cw = G.CL / 4;
+  for (int idx = threadIdx.x; idx < 16 * cw; idx += blockDim.x) {
+    const int g = idx / cw, t4 = 4 * (idx - g * cw);
+    const int u0 = G.CL + g - t4 - 3;  // bytes u0 .. u0+3 of wz, reversed
+    const uint32_t x = __funnelshift_r(wz[u0 >> 2], wz[(u0 >> 2) + 1], 8 * (u0 & 3));
+    T[idx] = __byte_perm(x, 0, 0x0123);
+  }
+}
+
+// |pa +/- pb| (pb may be null) of this thread's signal into operand row m of
+// the CTA (4L bytes, zero padded to Kpad); returns its sign (1 = negative).
+__device__ uint32_t tc_prep(TcCtx &c, const uint32_t *pa, const uint32_t *pb, size_t plane, bool sub, bool valid) {
+  const TcGeom &G = c.G;
+  const int L = G.L, m = threadIdx.x;
+  uint8_t *row = c.smem + (size_t)(m >> 3) * (8 * G.Kpad) + (m & 7) * 16;
+  const uint32_t msk = sub ? 0xffffffffu : 0u;
+  uint32_t cy = sub ? 1u : 0u, top = 0;
+  const int nch = G.Kpad / 16;
+  for (int ch = 0; ch < nch; ++ch) {
+    uint32_t w4[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = 4 * ch + e;
+      uint32_t v = 0;
+      if (valid && i < L) {
+        v = pb ? add_c(pa[(size_t)i * plane], pb[(size_t)i * plane] ^ msk, cy) : pa[(size_t)i * plane];
+        top = v;
+      }
+      w4[e] = v;
+    }
+    *reinterpret_cast<uint4 *>(row + ch * 128) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+  }
+  const uint32_t neg = top >> 31;
+  if (neg) {  // two's complement -> magnitude (limbs below L only)
+    uint32_t cc = 1;
+    for (int ch = 0; 4 * ch < L; ++ch) {
+      uint4 u = *reinterpret_cast<uint4 *>(row + ch * 128);
+      uint32_t w4[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (4 * ch + e < L) w4[e] = add_c(~w4[e], 0, cc);
+      *reinterpret_cast<uint4 *>(row + ch * 128) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+    }
+  }
+  return neg;
+}
+
+// thread 0: the MMAs of output tile t of twiddle `which` into buffer buf
+__device__ void tc_issue(const TcCtx &c, int which, int t, int buf) {
+  const TcGeom &G = c.G;
+  const int J = G.J0 + 128 * t;
+  const int s_lo = max(0, J - 4 * G.L + 1) >> 5;  // K steps that meet nonzero Toeplitz entries
+  const int s_hi = min(G.Kpad >> 5, (J + 159) >> 5);
+  const uint32_t tb = c.sT + (uint32_t)which * 16u * G.CL + (uint32_t)(G.Q - J - 112);
+  const uint32_t d = c.tmem + (uint32_t)buf * 128u;
+  for (int s = s_lo; s < s_hi; ++s)
+    tc_mma(d, tc_desc(c.sA + 256u * s, 128u, 8u * G.Kpad), tc_desc(tb + 32u * s, 16u, G.CL), kTcIdesc,
+           s > s_lo ? 1u : 0u);
+  tc_commit(c.bar + 8u * buf);
+}
+
+// Where a product's result limbs go:  dst[q] = sx*r_q + sp*P[q]  (streamed chains)
+struct TcEmit {
+  uint32_t *dst;
+  size_t ds;
+  const uint32_t *P;
+  size_t ps;
+  uint32_t rm, cr, pm, keep, cm;
+  bool on;
+  __device__ void init(bool valid, uint32_t xneg, bool negx, const uint32_t *P_, size_t ps_, int sp, uint32_t *dst_,
+                       size_t ds_) {
+    on = valid;
+    dst = dst_;
+    ds = ds_;
+    P = P_;
+    ps = ps_;
+    const bool rneg = (xneg != 0) != negx;
+    rm = rneg ? 0xffffffffu : 0u;
+    cr = rneg ? 1u : 0u;
+    pm = sp < 0 ? 0xffffffffu : 0u;
+    keep = sp != 0 ? 0xffffffffu : 0u;
+    cm = sp < 0 ? 1u : 0u;
+  }
+  __device__ __forceinline__ void put(int q, uint32_t r) {
+    if (!on) return;
+    const uint32_t rv = add_c(r ^ rm, 0, cr);
+    const uint32_t pv = P ? ((P[(size_t)q * ps] & keep) ^ pm) : 0u;
+    dst[(size_t)q * ds] = add_c(rv, pv, cm);
+  }
+};
+
+// One product per signal of the CTA: operand rows (already in shared memory,
+// made visible to the async proxy) times twiddle `which`; all threads.
+__device__ void tc_product(TcCtx &c, int which, TcEmit &em) {
+  const TcGeom &G = c.G;
+  const int L = G.L;
+  const uint32_t lane_addr = c.tmem + ((uint32_t)((threadIdx.x >> 5) * 32) << 16);
+  uint64_t acc = 0, carry = 0;
+  uint32_t prev = 0;
+  if (threadIdx.x == 0) {
+    tc_fence_after();
+    tc_issue(c, which, 0, c.counter & 1);
+  }
+  __syncwarp();
+  for (int t = 0; t < G.nt; ++t) {
+    const int buf = (c.counter + t) & 1;
+    if (threadIdx.x == 0 && t + 1 < G.nt) tc_issue(c, which, t + 1, buf ^ 1);
+    __syncwarp();
+    if (!c.bad && !mbar_wait(c.bar + 8u * buf, (c.ph >> buf) & 1u)) c.bad = true;
+    c.ph ^= 1u << buf;
+    tc_fence_after();
+    uint32_t v[128];
+    MPFFT_TMEM_LD32(lane_addr + buf * 128u + 0u, v);
+    MPFFT_TMEM_LD32(lane_addr + buf * 128u + 32u, v + 32);
+    MPFFT_TMEM_LD32(lane_addr + buf * 128u + 64u, v + 64);
+    MPFFT_TMEM_LD32(lane_addr + buf * 128u + 96u, v + 96);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    const int mbase = (G.J0 >> 2) + 32 * t;  // limb column of this tile's first byte column
+#pragma unroll
+    for (int jj = 0; jj < 128; ++jj) {
+      // output column J + jj sits in row n = 8 (jj mod 16) + 7 - jj/16 of the tile
+      acc += (uint64_t)v[8 * (jj & 15) + 7 - (jj >> 4)] << (8 * (jj & 3));
+      if ((jj & 3) == 3) {
+        const int m = mbase + (jj >> 2);
+        uint64_t s = acc + carry;
+        acc = 0;
+        if (m == L - 1) s += 1ull << 30;  // + 2^(32L-2): round to nearest
+        const uint32_t limb = (uint32_t)s;
+        carry = s >> 32;
+        const int q = m - L;
+        if (q >= 0 && q < L) em.put(q, __funnelshift_r(prev, limb, 31));
+        prev = limb;
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  c.counter += G.nt;
+}
+
+// ---------------------------------------------------------------------------
+// level kernel
+// ---------------------------------------------------------------------------
+
+// One CTA per (node, butterfly index k, group of 128 signals); the same six
+// steps as mp_big_level_kernel (3m3a products merged into the Z slots, then
+// the swapped L-combine).  Scratch: L limb planes of gridDim.x*128 words (the
+// first product of each side).
+__global__ void __launch_bounds__(kTcRows, 1)
+    mp_tc_level_kernel(uint32_t *__restrict__ y, int N, int B, int L, int n, const int *__restrict__ node_off,
+                       const uint32_t *__restrict__ tw, const uint8_t *__restrict__ dneg, int tws,
+                       uint32_t *__restrict__ scratch, int *err) {
+  extern __shared__ __align__(1024) uint8_t tc_smem[];
+  const int q = n >> 2;
+  const int nbg = (B + kTcRows - 1) / kTcRows;
+  long long cta = blockIdx.x;
+  const int bg = (int)(cta % nbg);
+  cta /= nbg;
+  const int k = (int)(cta % q);
+  const int off = node_off[cta / q];
+  const int b = bg * kTcRows + (int)threadIdx.x;
+  const bool valid = b < B;
+  const int bs = valid ? b : 0;
+  const size_t plane = (size_t)N * B;
+  const size_t cim = (size_t)L * plane;
+  uint32_t *u0 = y + (size_t)(off + k) * B + bs;
+  uint32_t *u1 = u0 + (size_t)q * B;
+  uint32_t *zp = u0 + (size_t)2 * q * B;
+  uint32_t *zm = u0 + (size_t)3 * q * B;
+  if (k == 0) {  // no twiddle products
+    if (valid) big_combine(u0, u1, zp, zm, plane, cim, L, false);
+    return;
+  }
+  TcCtx c;
+  tc_setup(c, tc_smem, L);
+  const size_t tplane = (size_t)(N >> 2) * tws;
+  const int kn = k * (N / n) * tws;
+  const bool special = 2 * k == q;
+  const bool dn = special ? false : (dneg[kn] != 0);
+  for (int which = 0; which < (special ? 1 : 3); ++which)
+    tc_build_twiddle(c, which, tw + (size_t)which * L * tplane + kn, tplane);
+  const size_t ss = (size_t)gridDim.x * kTcRows;  // scratch limb-plane stride
+  uint32_t *P = scratch + (size_t)blockIdx.x * kTcRows + threadIdx.x;
+  for (int st_ = 0; st_ < 6; ++st_) {
+    const int side = st_ >= 3;
+    const int step = st_ - 3 * side;
+    uint32_t *zr = side ? zm : zp;
+    uint32_t *zi = zr + cim;
+    const uint32_t *pa = zr, *pb = nullptr;
+    int which = 0;
+    bool sub = false, negx = false, mul = true;
+    int sp = 0;
+    uint32_t *dst = nullptr;
+    if (step == 0) {
+      pb = zi;
+      sub = side;
+    } else if (!special) {
+      if (step == 1) {
+        pa = zi;
+        which = 2;
+        negx = dn ^ (side == 0);
+        sp = 1;
+        dst = zi;
+      } else {
+        which = 1;
+        negx = side == 0;
+        sp = side ? -1 : 1;
+        dst = zr;
+      }
+    } else {
+      if (step == 1) {
+        pa = side ? zr : zi;
+        pb = side ? zi : zr;
+        sub = !side;
+        dst = zr;
+      } else {
+        mul = false;
+        dst = zi;
+      }
+    }
+    if (!mul) {
+      if (valid)
+        for (int i = 0; i < L; ++i) dst[(size_t)i * plane] = P[(size_t)i * ss];
+      continue;
+    }
+    const uint32_t xneg = tc_prep(c, pa, pb, plane, sub, valid);
+    fence_async_smem();
+    __syncthreads();
+    TcEmit em;
+    if (!dst) em.init(valid, xneg, false, nullptr, ss, 0, P, ss);
+    else em.init(valid, xneg, negx, P, ss, sp, dst, plane);
+    tc_product(c, which, em);
+  }
+  if (valid) big_combine(u0, u1, zp, zm, plane, cim, L, true);
+  tc_teardown(c, err);
+}
+
+// products of B operands (limb planes x[i*B + b], two's complement) with one
+// twiddle magnitude w[0 .. L-1]: out[i*B + b] = sign(x) * r (diagnostics)
+__global__ void __launch_bounds__(kTcRows, 1)
+    mp_tc_mul_kernel(const uint32_t *__restrict__ x, const uint32_t *__restrict__ w, uint32_t *__restrict__ out,
+                     int L, int B, int *err) {
+  extern __shared__ __align__(1024) uint8_t tc_smem[];
+  const int b = blockIdx.x * kTcRows + (int)threadIdx.x;
+  const bool valid = b < B;
+  const int bs = valid ? b : 0;
+  TcCtx c;
+  tc_setup(c, tc_smem, L);
+  tc_build_twiddle(c, 0, w, 1);
+  const uint32_t xneg = tc_prep(c, x + bs, nullptr, (size_t)B, false, valid);
+  fence_async_smem();
+  __syncthreads();
+  TcEmit em;
+  em.init(valid, xneg, false, nullptr, 0, 0, out + bs, (size_t)B);
+  tc_product(c, 0, em);
+  tc_teardown(c, err);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+static cudaError_t tc_prepare(const void *fn, uint32_t bytes, int **err) {
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return e;
+  return cudaGetSymbolAddress(reinterpret_cast<void **>(err), g_tc_error);
+}
+
+size_t mp_tc_scratch_words(const MpDeviceTables &T, int L, int B) {
+  long long most = 0;
+  const long long nbg = (B + kTcRows - 1) / kTcRows;
+  for (int lv = 0; lv < T.nlevels; ++lv) {
+    const long long th = (long long)T.level_count[lv] * (T.level_n[lv] / 4) * nbg * kTcRows;
+    if (th > most) most = th;
+  }
+  return (size_t)L * (size_t)most;
+}
+
+cudaError_t mp_tc_run_levels(int L, const MpDeviceTables &T, uint32_t *out, int B, uint32_t *scratch,
+                             cudaStream_t s, LaunchTimer &timer) {
+  const TcGeom G = tc_geom(L);
+  int *err = nullptr;
+  cudaError_t e = tc_prepare((const void *)mp_tc_level_kernel, G.bytes, &err);
+  if (e != cudaSuccess) return e;
+  const long long nbg = (B + kTcRows - 1) / kTcRows;
+  for (int lv = 0; lv < T.nlevels; ++lv) {
+    const int n = T.level_n[lv];
+    const long long ctas = (long long)T.level_count[lv] * (n / 4) * nbg;
+    timer.begin();
+    mp_tc_level_kernel<<<(unsigned)ctas, kTcRows, G.bytes, s>>>(out, T.N, B, L, n, T.node_off + T.level_start[lv],
+                                                               T.tw, T.dneg, T.tws, scratch, err);
+    timer.end();
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t mp_tc_mul(int L, int B, const uint32_t *x, const uint32_t *w, uint32_t *out, cudaStream_t s) {
+  const TcGeom G = tc_geom(L);
+  int *err = nullptr;
+  cudaError_t e = tc_prepare((const void *)mp_tc_mul_kernel, G.bytes, &err);
+  if (e != cudaSuccess) return e;
+  mp_tc_mul_kernel<<<(B + kTcRows - 1) / kTcRows, kTcRows, G.bytes, s>>>(x, w, out, L, B, err);
+  return cudaGetLastError();
+}
+
+cudaError_t mp_tc_take_error(int *code) {
+  int *err = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&err), g_tc_error);
+  if (e != cudaSuccess) return e;
+  const int zero = 0;
+  if ((e = cudaMemcpy(code, err, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return e;
+  return cudaMemcpy(err, &zero, sizeof(int), cudaMemcpyHostToDevice);
+}
+
+size_t mp_tc_smem_bytes(int L) { return tc_geom(L).bytes; }
+
+}  // namespace mpfft

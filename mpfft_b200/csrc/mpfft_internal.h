@@ -40,6 +40,7 @@ struct MpDeviceTables : TreeTables {
   const uint32_t *tw = nullptr;   // [3][L][tws*N/4]: cos, cos+sin, |cos-sin| magnitudes
   const uint8_t *dneg = nullptr;  // [tws*N/4]: sign of cos-sin
   int tws = 1;  // the table is built for tws*N points (2 for a real transform of 2N points)
+  int tc = 1;   // large limb counts: twiddle products on the tensor cores (mp_tc_kernels.cu)
 };
 
 // Schedule of one shared-memory sub-transform of size `size` (FP64 tier):
@@ -94,6 +95,10 @@ struct MpPlanView {
 constexpr int kMaxLimbs = 34;
 constexpr int kMaxLimbsBig = 520;
 constexpr int kMinLimbs = 2;
+// limb counts whose level kernels run their twiddle products as int8 tensor-core
+// GEMMs (P from about 2000 to 8200 bits at N = 1024)
+constexpr int kTcMinLimbs = 64;
+constexpr int kTcMaxLimbs = 260;
 
 // launch_ms (optional, host array of >= 1 + nlevels floats): when non-null,
 // each launch is bracketed by events on `s` and its duration written there
@@ -135,6 +140,17 @@ size_t mp_big_scratch_words(const MpDeviceTables &T, int L, int B);
 cudaError_t mp_big_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
                                  uint32_t *scratch, cudaStream_t s, float *launch_ms);
 cudaError_t diag_imad_rate(int wide, double *ops_per_s);
+// tensor-core level kernels (kTcMinLimbs <= L <= kTcMaxLimbs); scratch of
+// mp_tc_scratch_words words
+size_t mp_tc_scratch_words(const MpDeviceTables &T, int L, int B);
+cudaError_t mp_tc_run_levels(int L, const MpDeviceTables &T, uint32_t *out, int B, uint32_t *scratch, cudaStream_t s,
+                             LaunchTimer &timer);
+// diagnostics: B signed products x * w through the tensor-core product
+cudaError_t mp_tc_mul(int L, int B, const uint32_t *x, const uint32_t *w, uint32_t *out, cudaStream_t s);
+// reads and clears the device-side error flag of the tensor-core kernels
+cudaError_t mp_tc_take_error(int *code);
+size_t mp_tc_smem_bytes(int L);
+inline bool mp_tc_used(const MpDeviceTables &T, int L) { return T.tc && L >= kTcMinLimbs && L <= kTcMaxLimbs; }
 // Split step of a real transform of 2M points (L <= kMaxLimbs; tw/dneg: the
 // table of a 2M-point plan).  forward: Z (M points) -> 2X (M+1 points);
 // otherwise half spectrum X (M+1 points) -> 2Z with its planes exchanged.
