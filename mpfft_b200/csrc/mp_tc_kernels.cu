@@ -219,20 +219,27 @@ __device__ uint32_t tc_prep(TcCtx &c, const uint32_t *pa, const uint32_t *pb, si
   uint8_t *row = c.smem + (size_t)(m >> 3) * (8 * G.Kpad) + (m & 7) * 16;
   const uint32_t msk = sub ? 0xffffffffu : 0u;
   uint32_t cy = sub ? 1u : 0u, top = 0;
-  const int nch = G.Kpad / 16;
-  for (int ch = 0; ch < nch; ++ch) {
-    uint32_t w4[4];
+  const int nch = G.Kpad / 16;  // even: Kpad is a multiple of 32
+  for (int ch = 0; ch < nch; ch += 2) {
+    // 8 limbs of each input in flight before the carry chain consumes them
+    uint32_t va[8], vb[8];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < 8; ++e) {
       const int i = 4 * ch + e;
-      uint32_t v = 0;
-      if (valid && i < L) {
-        v = pb ? add_c(pa[(size_t)i * plane], pb[(size_t)i * plane] ^ msk, cy) : pa[(size_t)i * plane];
-        top = v;
-      }
-      w4[e] = v;
+      const bool in = valid && i < L;
+      va[e] = in ? pa[(size_t)i * plane] : 0u;
+      vb[e] = (in && pb) ? pb[(size_t)i * plane] : 0u;
     }
-    *reinterpret_cast<uint4 *>(row + ch * 128) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int i = 4 * ch + e;
+      if (valid && i < L) {
+        va[e] = pb ? add_c(va[e], vb[e] ^ msk, cy) : va[e];
+        top = va[e];
+      }
+    }
+    *reinterpret_cast<uint4 *>(row + ch * 128) = make_uint4(va[0], va[1], va[2], va[3]);
+    *reinterpret_cast<uint4 *>(row + (ch + 1) * 128) = make_uint4(va[4], va[5], va[6], va[7]);
   }
   const uint32_t neg = top >> 31;
   if (neg) {  // two's complement -> magnitude (limbs below L only)
@@ -263,35 +270,105 @@ __device__ void tc_issue(const TcCtx &c, int which, int t, int buf) {
   tc_commit(c.bar + 8u * buf);
 }
 
-// Where a product's result limbs go:  dst[q] = sx*r_q + sp*P[q]  (streamed chains)
+// Where a product's result limbs go: dst[q] = sign * r_q (two's complement,
+// streamed; stores only, the merges happen in tc_combine)
 struct TcEmit {
   uint32_t *dst;
   size_t ds;
-  const uint32_t *P;
-  size_t ps;
-  uint32_t rm, cr, pm, keep, cm;
+  uint32_t rm, cr;
   bool on;
-  __device__ void init(bool valid, uint32_t xneg, bool negx, const uint32_t *P_, size_t ps_, int sp, uint32_t *dst_,
-                       size_t ds_) {
+  __device__ void init(bool valid, uint32_t neg, uint32_t *dst_, size_t ds_) {
     on = valid;
     dst = dst_;
     ds = ds_;
-    P = P_;
-    ps = ps_;
-    const bool rneg = (xneg != 0) != negx;
-    rm = rneg ? 0xffffffffu : 0u;
-    cr = rneg ? 1u : 0u;
-    pm = sp < 0 ? 0xffffffffu : 0u;
-    keep = sp != 0 ? 0xffffffffu : 0u;
-    cm = sp < 0 ? 1u : 0u;
+    rm = neg ? 0xffffffffu : 0u;
+    cr = neg ? 1u : 0u;
   }
   __device__ __forceinline__ void put(int q, uint32_t r) {
     if (!on) return;
-    const uint32_t rv = add_c(r ^ rm, 0, cr);
-    const uint32_t pv = P ? ((P[(size_t)q * ps] & keep) ^ pm) : 0u;
-    dst[(size_t)q * ds] = add_c(rv, pv, cm);
+    dst[(size_t)q * ds] = add_c(r ^ rm, 0, cr);
   }
 };
+
+// The 3m3a merges and the L-combine in one streamed pass, 4 limbs of all
+// inputs in flight at a time.  Per side (Z+ in zp, Z- in zm) the twiddled
+// value is
+//     T_r = a_r P + b_r S_r,   T_i = a_i P + b_i S_i      (coefficients in {-1, 0, 1})
+// with P the side's first product and S_r, S_i the side's two slots read as
+// (imaginary, real) when `swapped` (the products' layout) or (real,
+// imaginary) otherwise.  Then the outputs of mp_kernels.cu combine():
+//     u0 = U0 + (T+ + T-),  zp = U0 - (T+ + T-),
+//     u1 = U1 - i (T+ - T-), zm = U1 + i (T+ - T-).
+struct TcSide {
+  const uint32_t *P;  // may be null when a_r = a_i = 0
+  int ar, br, ai, bi;
+};
+
+__device__ __forceinline__ uint32_t coef_mask(int a) { return a < 0 ? 0xffffffffu : 0u; }
+__device__ __forceinline__ uint32_t coef_keep(int a) { return a != 0 ? 0xffffffffu : 0u; }
+
+__device__ void tc_combine(uint32_t *u0, uint32_t *u1, uint32_t *zp, uint32_t *zm, size_t plane, size_t cim,
+                           size_t ps, int L, bool swapped, const TcSide &sp, const TcSide &sm) {
+  const size_t sre = swapped ? cim : 0, sim = swapped ? 0 : cim;
+  // merge chains: T+r, T+i, T-r, T-i
+  const TcSide *sd[2] = {&sp, &sm};
+  uint32_t kP[2][2], mP[2][2], kS[2][2], mS[2][2], cT[2][2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int a[2] = {sd[h]->ar, sd[h]->ai}, bb[2] = {sd[h]->br, sd[h]->bi};
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      kP[h][c] = coef_keep(a[c]);
+      mP[h][c] = coef_mask(a[c]);
+      kS[h][c] = coef_keep(bb[c]);
+      mS[h][c] = coef_mask(bb[c]);
+      cT[h][c] = (a[c] < 0 ? 1u : 0u) + (bb[c] < 0 ? 1u : 0u);
+    }
+  }
+  const bool hasP0 = sp.P != nullptr, hasP1 = sm.P != nullptr;
+  uint32_t ca1r = 0, ca1i = 0, ca2r = 1, ca2i = 1;
+  uint32_t c0r = 0, c2r = 1, c1r = 0, c3r = 1, c0i = 0, c2i = 1, c1i = 1, c3i = 0;
+  constexpr int U = 4;
+  for (int i0 = 0; i0 < L; i0 += U) {
+    uint32_t U0r[U], U0i[U], U1r[U], U1i[U], Ar[U], Ai[U], Br[U], Bi[U], P0[U], P1[U];
+#pragma unroll
+    for (int e = 0; e < U; ++e) {
+      const int i = i0 + e;
+      const bool in = i < L;
+      const size_t o = (size_t)(in ? i : 0) * plane;
+      U0r[e] = in ? u0[o] : 0u;
+      U0i[e] = in ? u0[o + cim] : 0u;
+      U1r[e] = in ? u1[o] : 0u;
+      U1i[e] = in ? u1[o + cim] : 0u;
+      Ar[e] = in ? zp[o + sre] : 0u;
+      Ai[e] = in ? zp[o + sim] : 0u;
+      Br[e] = in ? zm[o + sre] : 0u;
+      Bi[e] = in ? zm[o + sim] : 0u;
+      P0[e] = (in && hasP0) ? sp.P[(size_t)i * ps] : 0u;
+      P1[e] = (in && hasP1) ? sm.P[(size_t)i * ps] : 0u;
+    }
+#pragma unroll
+    for (int e = 0; e < U; ++e) {
+      const int i = i0 + e;
+      if (i >= L) break;
+      const size_t o = (size_t)i * plane;
+      const uint32_t m1r = add_c((P0[e] & kP[0][0]) ^ mP[0][0], (Ar[e] & kS[0][0]) ^ mS[0][0], cT[0][0]);
+      const uint32_t m1i = add_c((P0[e] & kP[0][1]) ^ mP[0][1], (Ai[e] & kS[0][1]) ^ mS[0][1], cT[0][1]);
+      const uint32_t m2r = add_c((P1[e] & kP[1][0]) ^ mP[1][0], (Br[e] & kS[1][0]) ^ mS[1][0], cT[1][0]);
+      const uint32_t m2i = add_c((P1[e] & kP[1][1]) ^ mP[1][1], (Bi[e] & kS[1][1]) ^ mS[1][1], cT[1][1]);
+      const uint32_t a1r = add_c(m1r, m2r, ca1r), a1i = add_c(m1i, m2i, ca1i);
+      const uint32_t a2r = add_c(m1r, ~m2r, ca2r), a2i = add_c(m1i, ~m2i, ca2i);
+      u0[o] = add_c(U0r[e], a1r, c0r);
+      zp[o] = add_c(U0r[e], ~a1r, c2r);
+      u1[o] = add_c(U1r[e], a2i, c1r);
+      zm[o] = add_c(U1r[e], ~a2i, c3r);
+      u0[o + cim] = add_c(U0i[e], a1i, c0i);
+      zp[o + cim] = add_c(U0i[e], ~a1i, c2i);
+      u1[o + cim] = add_c(U1i[e], ~a2r, c1i);
+      zm[o + cim] = add_c(U1i[e], a2r, c3i);
+    }
+  }
+}
 
 // One product per signal of the CTA: operand rows (already in shared memory,
 // made visible to the async proxy) times twiddle `which`; all threads.
@@ -346,10 +423,11 @@ __device__ void tc_product(TcCtx &c, int which, TcEmit &em) {
 // level kernel
 // ---------------------------------------------------------------------------
 
-// One CTA per (node, butterfly index k, group of 128 signals); the same six
-// steps as mp_big_level_kernel (3m3a products merged into the Z slots, then
-// the swapped L-combine).  Scratch: L limb planes of gridDim.x*128 words (the
-// first product of each side).
+// One CTA per (node, butterfly index k, group of 128 signals): the 3m3a
+// products of mp_big_level_kernel (three per side, two at k = n/8) on the
+// tensor cores, stored unmerged, then one streamed merge + L-combine pass.
+// Scratch: 2L limb planes of gridDim.x*128 words (the first product of each
+// side).
 __global__ void __launch_bounds__(kTcRows, 1)
     mp_tc_level_kernel(uint32_t *__restrict__ y, int N, int B, int L, int n, const int *__restrict__ node_off,
                        const uint32_t *__restrict__ tw, const uint8_t *__restrict__ dneg, int tws,
@@ -371,8 +449,9 @@ __global__ void __launch_bounds__(kTcRows, 1)
   uint32_t *u1 = u0 + (size_t)q * B;
   uint32_t *zp = u0 + (size_t)2 * q * B;
   uint32_t *zm = u0 + (size_t)3 * q * B;
-  if (k == 0) {  // no twiddle products
-    if (valid) big_combine(u0, u1, zp, zm, plane, cim, L, false);
+  if (k == 0) {  // no twiddle products: T = Z
+    const TcSide id{nullptr, 0, 1, 0, 1};
+    if (valid) tc_combine(u0, u1, zp, zm, plane, cim, 0, L, false, id, id);
     return;
   }
   TcCtx c;
@@ -384,58 +463,60 @@ __global__ void __launch_bounds__(kTcRows, 1)
   for (int which = 0; which < (special ? 1 : 3); ++which)
     tc_build_twiddle(c, which, tw + (size_t)which * L * tplane + kn, tplane);
   const size_t ss = (size_t)gridDim.x * kTcRows;  // scratch limb-plane stride
-  uint32_t *P = scratch + (size_t)blockIdx.x * kTcRows + threadIdx.x;
-  for (int st_ = 0; st_ < 6; ++st_) {
-    const int side = st_ >= 3;
-    const int step = st_ - 3 * side;
+  uint32_t *P0 = scratch + (size_t)blockIdx.x * kTcRows + threadIdx.x;  // first product of Z+
+  uint32_t *P1 = P0 + (size_t)L * ss;                                      // first product of Z-
+  // Products of each side (as the steps of mp_big_level_kernel, but unmerged):
+  //   P = c (Zr +/- Zi) -> scratch;  R1 = |cos-sin| Zi -> zi slot;  R2 = (cos+sin) Zr -> zr slot
+  // k = n/8: P = c (Zr +/- Zi) -> scratch, R = c (Zi - Zr) resp. c (Zr + Zi) -> zr slot.
+  for (int side = 0; side < 2; ++side) {
     uint32_t *zr = side ? zm : zp;
     uint32_t *zi = zr + cim;
-    const uint32_t *pa = zr, *pb = nullptr;
-    int which = 0;
-    bool sub = false, negx = false, mul = true;
-    int sp = 0;
-    uint32_t *dst = nullptr;
-    if (step == 0) {
-      pb = zi;
-      sub = side;
-    } else if (!special) {
-      if (step == 1) {
-        pa = zi;
-        which = 2;
-        negx = dn ^ (side == 0);
-        sp = 1;
-        dst = zi;
-      } else {
-        which = 1;
-        negx = side == 0;
-        sp = side ? -1 : 1;
-        dst = zr;
-      }
-    } else {
-      if (step == 1) {
+    uint32_t *Pd = side ? P1 : P0;
+    for (int step = 0; step < (special ? 2 : 3); ++step) {
+      const uint32_t *pa = zr, *pb = nullptr;
+      bool sub = false;
+      int which = 0;
+      uint32_t *dst = Pd;
+      size_t ds = ss;
+      if (step == 0) {
+        pb = zi;
+        sub = side;
+      } else if (special) {
         pa = side ? zr : zi;
         pb = side ? zi : zr;
         sub = !side;
         dst = zr;
-      } else {
-        mul = false;
+        ds = plane;
+      } else if (step == 1) {
+        pa = zi;
+        which = 2;
         dst = zi;
+        ds = plane;
+      } else {
+        which = 1;
+        dst = zr;
+        ds = plane;
       }
+      const uint32_t xneg = tc_prep(c, pa, pb, plane, sub, valid);
+      fence_async_smem();
+      __syncthreads();
+      TcEmit em;
+      em.init(valid, xneg, dst, ds);
+      tc_product(c, which, em);
     }
-    if (!mul) {
-      if (valid)
-        for (int i = 0; i < L; ++i) dst[(size_t)i * plane] = P[(size_t)i * ss];
-      continue;
-    }
-    const uint32_t xneg = tc_prep(c, pa, pb, plane, sub, valid);
-    fence_async_smem();
-    __syncthreads();
-    TcEmit em;
-    if (!dst) em.init(valid, xneg, false, nullptr, ss, 0, P, ss);
-    else em.init(valid, xneg, negx, P, ss, sp, dst, plane);
-    tc_product(c, which, em);
   }
-  if (valid) big_combine(u0, u1, zp, zm, plane, cim, L, true);
+  // merge coefficients (T_r from the zi slot, T_i from the zr slot):
+  //   Z+: T_r = P + (dn ? R1 : -R1), T_i = P - R2;   Z-: T_r = P + (dn ? -R1 : R1), T_i = R2 - P
+  //   k = n/8: T_r = P, T_i = R
+  TcSide s0, s1;
+  if (special) {
+    s0 = TcSide{P0, 1, 0, 0, 1};
+    s1 = TcSide{P1, 1, 0, 0, 1};
+  } else {
+    s0 = TcSide{P0, 1, dn ? 1 : -1, 1, -1};
+    s1 = TcSide{P1, 1, dn ? -1 : 1, -1, 1};
+  }
+  if (valid) tc_combine(u0, u1, zp, zm, plane, cim, ss, L, true, s0, s1);
   tc_teardown(c, err);
 }
 
@@ -455,7 +536,7 @@ __global__ void __launch_bounds__(kTcRows, 1)
   fence_async_smem();
   __syncthreads();
   TcEmit em;
-  em.init(valid, xneg, false, nullptr, 0, 0, out + bs, (size_t)B);
+  em.init(valid, xneg, out + bs, (size_t)B);
   tc_product(c, 0, em);
   tc_teardown(c, err);
 }
@@ -477,7 +558,7 @@ size_t mp_tc_scratch_words(const MpDeviceTables &T, int L, int B) {
     const long long th = (long long)T.level_count[lv] * (T.level_n[lv] / 4) * nbg * kTcRows;
     if (th > most) most = th;
   }
-  return (size_t)L * (size_t)most;
+  return (size_t)2 * L * (size_t)most;
 }
 
 cudaError_t mp_tc_run_levels(int L, const MpDeviceTables &T, uint32_t *out, int B, uint32_t *scratch,
