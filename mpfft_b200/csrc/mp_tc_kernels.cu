@@ -213,44 +213,68 @@ __device__ void tc_build_twiddle(TcCtx &c, int which, const uint32_t *w, size_t 
 
 // |pa +/- pb| (pb may be null) of this thread's signal into operand row m of
 // the CTA (4L bytes, zero padded to Kpad); returns its sign (1 = negative).
-__device__ uint32_t tc_prep(TcCtx &c, const uint32_t *pa, const uint32_t *pb, size_t plane, bool sub, bool valid) {
+// Rows of signals beyond the batch read signal 0 (the caller clamps the
+// pointers); their products are never stored.  Loads are unconditional, 8
+// limbs of each input in flight.
+__device__ uint32_t tc_prep(TcCtx &c, const uint32_t *pa, const uint32_t *pb, size_t plane, bool sub) {
   const TcGeom &G = c.G;
   const int L = G.L, m = threadIdx.x;
   uint8_t *row = c.smem + (size_t)(m >> 3) * (8 * G.Kpad) + (m & 7) * 16;
+  const bool two = pb != nullptr;
+  const uint32_t *qb = two ? pb : pa;
   const uint32_t msk = sub ? 0xffffffffu : 0u;
-  uint32_t cy = sub ? 1u : 0u, top = 0;
-  const int nch = G.Kpad / 16;  // even: Kpad is a multiple of 32
-  for (int ch = 0; ch < nch; ch += 2) {
-    // 8 limbs of each input in flight before the carry chain consumes them
+  uint32_t cy = sub ? 1u : 0u, last = 0;
+  int i0 = 0;
+  for (; i0 + 8 <= L; i0 += 8) {
     uint32_t va[8], vb[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
-      const int i = 4 * ch + e;
-      const bool in = valid && i < L;
-      va[e] = in ? pa[(size_t)i * plane] : 0u;
-      vb[e] = (in && pb) ? pb[(size_t)i * plane] : 0u;
+      va[e] = pa[(size_t)(i0 + e) * plane];
+      vb[e] = qb[(size_t)(i0 + e) * plane];
     }
+    if (two) {
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int i = 4 * ch + e;
-      if (valid && i < L) {
-        va[e] = pb ? add_c(va[e], vb[e] ^ msk, cy) : va[e];
-        top = va[e];
-      }
+      for (int e = 0; e < 8; ++e) va[e] = add_c(va[e], vb[e] ^ msk, cy);
     }
-    *reinterpret_cast<uint4 *>(row + ch * 128) = make_uint4(va[0], va[1], va[2], va[3]);
-    *reinterpret_cast<uint4 *>(row + (ch + 1) * 128) = make_uint4(va[4], va[5], va[6], va[7]);
+    last = va[7];
+    *reinterpret_cast<uint4 *>(row + (i0 >> 2) * 128) = make_uint4(va[0], va[1], va[2], va[3]);
+    *reinterpret_cast<uint4 *>(row + ((i0 >> 2) + 1) * 128) = make_uint4(va[4], va[5], va[6], va[7]);
   }
-  const uint32_t neg = top >> 31;
-  if (neg) {  // two's complement -> magnitude (limbs below L only)
+  // tail (fewer than 8 limbs) and zero padding up to Kpad, one 16-byte chunk at a time
+  for (int ch = i0 >> 2; ch < G.Kpad / 16; ++ch) {
+    uint32_t w4[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = 4 * ch + e;
+      uint32_t v = 0;
+      if (i < L) {
+        v = pa[(size_t)i * plane];
+        if (two) v = add_c(v, qb[(size_t)i * plane] ^ msk, cy);
+        last = v;
+      }
+      w4[e] = v;
+    }
+    *reinterpret_cast<uint4 *>(row + ch * 128) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+  }
+  const uint32_t neg = last >> 31;
+  if (neg) {  // two's complement -> magnitude (limbs below L only; the padding stays zero)
     uint32_t cc = 1;
-    for (int ch = 0; 4 * ch < L; ++ch) {
+    const int nfull = L >> 2;
+    for (int ch = 0; ch < nfull; ++ch) {
       uint4 u = *reinterpret_cast<uint4 *>(row + ch * 128);
+      u.x = add_c(~u.x, 0, cc);
+      u.y = add_c(~u.y, 0, cc);
+      u.z = add_c(~u.z, 0, cc);
+      u.w = add_c(~u.w, 0, cc);
+      *reinterpret_cast<uint4 *>(row + ch * 128) = u;
+    }
+    if (L & 3) {
+      uint4 u = *reinterpret_cast<uint4 *>(row + nfull * 128);
       uint32_t w4[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e)
-        if (4 * ch + e < L) w4[e] = add_c(~w4[e], 0, cc);
-      *reinterpret_cast<uint4 *>(row + ch * 128) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        if (e < (L & 3)) w4[e] = add_c(~w4[e], 0, cc);
+      *reinterpret_cast<uint4 *>(row + nfull * 128) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
     }
   }
   return neg;
@@ -325,7 +349,9 @@ __device__ void tc_combine(uint32_t *u0, uint32_t *u1, uint32_t *zp, uint32_t *z
       cT[h][c] = (a[c] < 0 ? 1u : 0u) + (bb[c] < 0 ? 1u : 0u);
     }
   }
-  const bool hasP0 = sp.P != nullptr, hasP1 = sm.P != nullptr;
+  // without a first product the coefficient of P is 0: read any valid word instead
+  const uint32_t *p0 = sp.P ? sp.P : u0, *p1 = sm.P ? sm.P : u0;
+  const size_t ps0 = sp.P ? ps : plane, ps1 = sm.P ? ps : plane;
   uint32_t ca1r = 0, ca1i = 0, ca2r = 1, ca2i = 1;
   uint32_t c0r = 0, c2r = 1, c1r = 0, c3r = 1, c0i = 0, c2i = 1, c1i = 1, c3i = 0;
   constexpr int U = 4;
@@ -333,19 +359,18 @@ __device__ void tc_combine(uint32_t *u0, uint32_t *u1, uint32_t *zp, uint32_t *z
     uint32_t U0r[U], U0i[U], U1r[U], U1i[U], Ar[U], Ai[U], Br[U], Bi[U], P0[U], P1[U];
 #pragma unroll
     for (int e = 0; e < U; ++e) {
-      const int i = i0 + e;
-      const bool in = i < L;
-      const size_t o = (size_t)(in ? i : 0) * plane;
-      U0r[e] = in ? u0[o] : 0u;
-      U0i[e] = in ? u0[o + cim] : 0u;
-      U1r[e] = in ? u1[o] : 0u;
-      U1i[e] = in ? u1[o + cim] : 0u;
-      Ar[e] = in ? zp[o + sre] : 0u;
-      Ai[e] = in ? zp[o + sim] : 0u;
-      Br[e] = in ? zm[o + sre] : 0u;
-      Bi[e] = in ? zm[o + sim] : 0u;
-      P0[e] = (in && hasP0) ? sp.P[(size_t)i * ps] : 0u;
-      P1[e] = (in && hasP1) ? sm.P[(size_t)i * ps] : 0u;
+      const int i = min(i0 + e, L - 1);  // tail: re-read the top limb, not stored
+      const size_t o = (size_t)i * plane;
+      U0r[e] = u0[o];
+      U0i[e] = u0[o + cim];
+      U1r[e] = u1[o];
+      U1i[e] = u1[o + cim];
+      Ar[e] = zp[o + sre];
+      Ai[e] = zp[o + sim];
+      Br[e] = zm[o + sre];
+      Bi[e] = zm[o + sim];
+      P0[e] = p0[(size_t)i * ps0];
+      P1[e] = p1[(size_t)i * ps1];
     }
 #pragma unroll
     for (int e = 0; e < U; ++e) {
@@ -497,7 +522,7 @@ __global__ void __launch_bounds__(kTcRows, 1)
         dst = zr;
         ds = plane;
       }
-      const uint32_t xneg = tc_prep(c, pa, pb, plane, sub, valid);
+      const uint32_t xneg = tc_prep(c, pa, pb, plane, sub);
       fence_async_smem();
       __syncthreads();
       TcEmit em;
@@ -532,7 +557,7 @@ __global__ void __launch_bounds__(kTcRows, 1)
   TcCtx c;
   tc_setup(c, tc_smem, L);
   tc_build_twiddle(c, 0, w, 1);
-  const uint32_t xneg = tc_prep(c, x + bs, nullptr, (size_t)B, false, valid);
+  const uint32_t xneg = tc_prep(c, x + bs, nullptr, (size_t)B, false);
   fence_async_smem();
   __syncthreads();
   TcEmit em;
