@@ -55,7 +55,7 @@ extern "C" {
 #define MPFFT_PLAN_HOST_ONLY 2u /* plan creation: conversion (pack/unpack) only, no device state */
 #define MPFFT_PLAN_HOST_CONVERSION 4u /* plan creation: convert mpfr_t <-> limbs on the host, not the GPU */
 #define MPFFT_PLAN_NO_TENSOR 16u /* plan creation: keep large-precision twiddle products on the integer
-                                     pipes (by default 64..260 limbs use int8 tensor-core GEMMs) */
+                                     pipes (by default 35..260 limbs use int8 tensor-core GEMMs) */
 
 /* ------------------------------------------------------------------------ */
 /* 1. drop-in replacements for mpFFT.h                                      */
@@ -235,7 +235,7 @@ int mpfft_diag_imad_rate(int wide, double *ops_per_s);
  * operands x (device limb planes x[i*batch + b], two's complement, L limbs,
  * |x| < 2^(32L-2)) and one unsigned twiddle w[0..L-1], with
  * r = floor((S + 2^(32L-2)) / 2^(32L-1)), S = the part of |x|*w in byte
- * columns >= 4L-8 rounded down to a multiple of 16.  64 <= L <= 260.
+ * columns >= 4L-8 rounded down to a multiple of 16.  35 <= L <= 260.
  * Asynchronous on `stream`. */
 int mpfft_diag_tc_mul(int limbs, unsigned long batch, const uint32_t *d_x, const uint32_t *d_w, uint32_t *d_out,
                       void *stream);

@@ -1,7 +1,7 @@
 // Multiprecision butterflies whose twiddle products run on the tensor cores
 // (tcgen05.mma kind::i8: unsigned 8-bit operands, exact int32 accumulation
 // in tensor memory), for large limb counts kTcMinLimbs <= L <= kTcMaxLimbs
-// (P from about 2000 to 8200 bits).
+// (P from about 1050 to 8200 bits at N = 1024).
 //
 // Product as a matrix product.  At one level and one butterfly index k every
 // signal multiplies its operands by the same three twiddle constants (cos,
@@ -214,7 +214,7 @@ __device__ void tc_build_twiddle(TcCtx &c, int which, const uint32_t *w, size_t 
 // |pa +/- pb| (pb may be null) of this thread's signal into operand row m of
 // the CTA (4L bytes, zero padded to Kpad); returns its sign (1 = negative).
 // Rows of signals beyond the batch read signal 0 (the caller clamps the
-// pointers); their products are never stored.  Loads are unconditional, 8
+// pointers); their products are never stored.  Loads are unconditional, 16
 // limbs of each input in flight.
 __device__ uint32_t tc_prep(TcCtx &c, const uint32_t *pa, const uint32_t *pb, size_t plane, bool sub) {
   const TcGeom &G = c.G;
@@ -225,20 +225,23 @@ __device__ uint32_t tc_prep(TcCtx &c, const uint32_t *pa, const uint32_t *pb, si
   const uint32_t msk = sub ? 0xffffffffu : 0u;
   uint32_t cy = sub ? 1u : 0u, last = 0;
   int i0 = 0;
-  for (; i0 + 8 <= L; i0 += 8) {
-    uint32_t va[8], vb[8];
+  constexpr int kB = 16;
+  for (; i0 + kB <= L; i0 += kB) {
+    uint32_t va[kB], vb[kB];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
+    for (int e = 0; e < kB; ++e) {
       va[e] = pa[(size_t)(i0 + e) * plane];
       vb[e] = qb[(size_t)(i0 + e) * plane];
     }
     if (two) {
 #pragma unroll
-      for (int e = 0; e < 8; ++e) va[e] = add_c(va[e], vb[e] ^ msk, cy);
+      for (int e = 0; e < kB; ++e) va[e] = add_c(va[e], vb[e] ^ msk, cy);
     }
-    last = va[7];
-    *reinterpret_cast<uint4 *>(row + (i0 >> 2) * 128) = make_uint4(va[0], va[1], va[2], va[3]);
-    *reinterpret_cast<uint4 *>(row + ((i0 >> 2) + 1) * 128) = make_uint4(va[4], va[5], va[6], va[7]);
+    last = va[kB - 1];
+#pragma unroll
+    for (int q4 = 0; q4 < kB / 4; ++q4)
+      *reinterpret_cast<uint4 *>(row + ((i0 >> 2) + q4) * 128) =
+          make_uint4(va[4 * q4], va[4 * q4 + 1], va[4 * q4 + 2], va[4 * q4 + 3]);
   }
   // tail (fewer than 8 limbs) and zero padding up to Kpad, one 16-byte chunk at a time
   for (int ch = i0 >> 2; ch < G.Kpad / 16; ++ch) {
@@ -295,26 +298,27 @@ __device__ void tc_issue(const TcCtx &c, int which, int t, int buf) {
 }
 
 // Where a product's result limbs go: dst[q] = sign * r_q (two's complement,
-// streamed; stores only, the merges happen in tc_combine)
+// streamed in increasing q; stores only, the merges happen in tc_combine)
 struct TcEmit {
-  uint32_t *dst;
+  uint32_t *p;
   size_t ds;
   uint32_t rm, cr;
   bool on;
   __device__ void init(bool valid, uint32_t neg, uint32_t *dst_, size_t ds_) {
     on = valid;
-    dst = dst_;
+    p = dst_;
     ds = ds_;
     rm = neg ? 0xffffffffu : 0u;
     cr = neg ? 1u : 0u;
   }
-  __device__ __forceinline__ void put(int q, uint32_t r) {
-    if (!on) return;
-    dst[(size_t)q * ds] = add_c(r ^ rm, 0, cr);
+  __device__ __forceinline__ void put(uint32_t r) {
+    const uint32_t v = add_c(r ^ rm, 0, cr);
+    if (on) *p = v;
+    p += ds;
   }
 };
 
-// The 3m3a merges and the L-combine in one streamed pass, 4 limbs of all
+// The 3m3a merges and the L-combine in one streamed pass, 8 limbs of all
 // inputs in flight at a time.  Per side (Z+ in zp, Z- in zm) the twiddled
 // value is
 //     T_r = a_r P + b_r S_r,   T_i = a_i P + b_i S_i      (coefficients in {-1, 0, 1})
@@ -354,7 +358,7 @@ __device__ void tc_combine(uint32_t *u0, uint32_t *u1, uint32_t *zp, uint32_t *z
   const size_t ps0 = sp.P ? ps : plane, ps1 = sm.P ? ps : plane;
   uint32_t ca1r = 0, ca1i = 0, ca2r = 1, ca2i = 1;
   uint32_t c0r = 0, c2r = 1, c1r = 0, c3r = 1, c0i = 0, c2i = 1, c1i = 1, c3i = 0;
-  constexpr int U = 4;
+  constexpr int U = 8;
   for (int i0 = 0; i0 < L; i0 += U) {
     uint32_t U0r[U], U0i[U], U1r[U], U1i[U], Ar[U], Ai[U], Br[U], Bi[U], P0[U], P1[U];
 #pragma unroll
@@ -401,7 +405,7 @@ __device__ void tc_product(TcCtx &c, int which, TcEmit &em) {
   const TcGeom &G = c.G;
   const int L = G.L;
   const uint32_t lane_addr = c.tmem + ((uint32_t)((threadIdx.x >> 5) * 32) << 16);
-  uint64_t acc = 0, carry = 0;
+  uint64_t carry = 0;
   uint32_t prev = 0;
   if (threadIdx.x == 0) {
     tc_fence_after();
@@ -423,20 +427,20 @@ __device__ void tc_product(TcCtx &c, int which, TcEmit &em) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
     const int mbase = (G.J0 >> 2) + 32 * t;  // limb column of this tile's first byte column
 #pragma unroll
-    for (int jj = 0; jj < 128; ++jj) {
+    for (int lc = 0; lc < 32; ++lc) {
+      const int m = mbase + lc;
+      if (m >= 2 * L) break;  // above the product's top limb
       // output column J + jj sits in row n = 8 (jj mod 16) + 7 - jj/16 of the tile
-      acc += (uint64_t)v[8 * (jj & 15) + 7 - (jj >> 4)] << (8 * (jj & 3));
-      if ((jj & 3) == 3) {
-        const int m = mbase + (jj >> 2);
-        uint64_t s = acc + carry;
-        acc = 0;
-        if (m == L - 1) s += 1ull << 30;  // + 2^(32L-2): round to nearest
-        const uint32_t limb = (uint32_t)s;
-        carry = s >> 32;
-        const int q = m - L;
-        if (q >= 0 && q < L) em.put(q, __funnelshift_r(prev, limb, 31));
-        prev = limb;
-      }
+      uint64_t sum = carry;
+      sum += (uint64_t)v[8 * ((4 * lc) & 15) + 7 - ((4 * lc) >> 4)];
+      sum += (uint64_t)v[8 * ((4 * lc + 1) & 15) + 7 - ((4 * lc + 1) >> 4)] * 0x100u;
+      sum += (uint64_t)v[8 * ((4 * lc + 2) & 15) + 7 - ((4 * lc + 2) >> 4)] * 0x10000u;
+      sum += (uint64_t)v[8 * ((4 * lc + 3) & 15) + 7 - ((4 * lc + 3) >> 4)] * 0x1000000u;
+      if (m == L - 1) sum += 1ull << 30;  // + 2^(32L-2): round to nearest
+      const uint32_t limb = (uint32_t)sum;
+      carry = sum >> 32;
+      if (m >= L) em.put(__funnelshift_r(prev, limb, 31));  // result limb m - L
+      prev = limb;
     }
     tc_fence_before();
     __syncthreads();

@@ -96,8 +96,10 @@ constexpr int kMaxLimbs = 34;
 constexpr int kMaxLimbsBig = 520;
 constexpr int kMinLimbs = 2;
 // limb counts whose level kernels run their twiddle products as int8 tensor-core
-// GEMMs (P from about 2000 to 8200 bits at N = 1024)
-constexpr int kTcMinLimbs = 64;
+// GEMMs: every count above the register kernels up to 260 (P from about 1050
+// to 8200 bits at N = 1024); measured faster than the streaming integer kernels
+// over the whole range
+constexpr int kTcMinLimbs = 35;
 constexpr int kTcMaxLimbs = 260;
 
 // launch_ms (optional, host array of >= 1 + nlevels floats): when non-null,
