@@ -125,6 +125,18 @@ typedef struct mpfft_d_plan mpfft_d_plan;
 int mpfft_mp_plan_create(mpfft_mp_plan **plan, unsigned long n, long prec);
 /* same, with flags (MPFFT_PLAN_HOST_ONLY: pack/unpack only, needs no GPU) */
 int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, long prec, unsigned flags);
+/* Multi-dimensional transform (iterated one-dimensional transforms; the
+ * reference's README plans it but never built it): rank 1..3 dimensions
+ * dims[0] x ... x dims[rank-1], each a power of two, N = their product (at most
+ * 2^26).  A signal is N points in row-major order (last index fastest) in
+ * every layout this header describes: host arrays, device limb planes (point
+ * p = row-major index).  The limb format is that of an N-point plan; the
+ * error bound is that of an N-point transform.  Per axis the device first
+ * rotates that axis to the front (one transposition pass) and then runs the
+ * one-dimensional kernels over all lines; a device buffer the size of the
+ * signals is allocated on first use and kept.  flags as
+ * mpfft_mp_plan_create_flags. */
+int mpfft_mp_plan_create_nd(mpfft_mp_plan **plan, int rank, const unsigned long *dims, long prec, unsigned flags);
 int mpfft_mp_plan_destroy(mpfft_mp_plan *plan);
 /* device format of a plan: limbs per real component, fraction bits */
 int mpfft_mp_plan_limbs(const mpfft_mp_plan *plan);
@@ -178,6 +190,11 @@ int mpfft_mp_unpack(const mpfft_mp_plan *plan, unsigned long batch, const uint32
 
 /* FP64 plans.  Host arrays: signal b at [b*n, (b+1)*n) of each array. */
 int mpfft_d_plan_create(mpfft_d_plan **plan, unsigned long n);
+/* FP64 multi-dimensional plan (rank 1..3, row-major, at most 2^28 points): the
+ * reference's double transform along each axis in turn, last axis first,
+ * each bit-identical to d_sr24_cp_fft; layout [c][b][p] with p the row-major
+ * index.  MPFFT_SCALED multiplies by 1/N (exactly, one axis at a time). */
+int mpfft_d_plan_create_nd(mpfft_d_plan **plan, int rank, const unsigned long *dims);
 int mpfft_d_plan_destroy(mpfft_d_plan *plan);
 int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const double *inr, const double *ini, double *outr,
                     double *outi, unsigned flags);

@@ -69,6 +69,8 @@ def _load() -> C.CDLL:
         "mpfft_mp_execute": (C.c_int, [vp, ul, vp, vp, vp, vp, C.c_uint]),
         "mpfft_mp_execute_device": (C.c_int, [vp, ul, u32p, u32p, vp]),
         "mpfft_mp_plan_create_real": (C.c_int, [C.POINTER(vp), ul, sl, C.c_uint]),
+        "mpfft_mp_plan_create_nd": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(ul), sl, C.c_uint]),
+        "mpfft_d_plan_create_nd": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(ul)]),
         "mpfft_mp_execute_r2c": (C.c_int, [vp, ul, vp, vp, vp, C.c_uint]),
         "mpfft_mp_execute_c2r": (C.c_int, [vp, ul, vp, vp, vp, C.c_uint]),
         "mpfft_mp_pack": (C.c_int, [vp, ul, vp, vp, u32p, vp]),
@@ -224,6 +226,26 @@ class MpPlan:
         _check(lib.mpfft_mp_unpack(self.h, batch, planes_ptr, exps_ptr, outr, outi, SCALED if scaled else 0))
 
 
+class MpPlanND(MpPlan):
+    """Multiprecision multi-dimensional plan: dims (row-major, last fastest)."""
+
+    def __init__(self, dims, prec: int, host_only: bool = False, host_conversion: bool = False,
+                 tensor: bool = True):
+        h = C.c_void_p()
+        flags = ((PLAN_HOST_ONLY if host_only else 0) | (PLAN_HOST_CONVERSION if host_conversion else 0)
+                 | (0 if tensor else PLAN_NO_TENSOR))
+        d = (C.c_ulong * len(dims))(*dims)
+        _check(lib.mpfft_mp_plan_create_nd(C.byref(h), len(dims), d, prec, flags))
+        self.h = h
+        self.dims = tuple(dims)
+        self.n = 1
+        for v in dims:
+            self.n *= v
+        self.prec = prec
+        self.limbs = lib.mpfft_mp_plan_limbs(h)
+        self.frac_bits = lib.mpfft_mp_plan_frac_bits(h)
+
+
 class MpRealPlan:
     """Multiprecision real transform of n real points (n/2+1-point half spectrum)."""
 
@@ -288,3 +310,17 @@ class DPlan:
 
     def execute_device(self, batch, d_in: int, d_out: int, scaled=False, stream: int = 0) -> None:
         _check(lib.mpfft_d_execute_device(self.h, batch, d_in, d_out, SCALED if scaled else 0, stream or None))
+
+
+class DPlanND(DPlan):
+    """FP64 multi-dimensional plan: dims (row-major, last fastest)."""
+
+    def __init__(self, dims):
+        h = C.c_void_p()
+        d = (C.c_ulong * len(dims))(*dims)
+        _check(lib.mpfft_d_plan_create_nd(C.byref(h), len(dims), d))
+        self.h = h
+        self.dims = tuple(dims)
+        self.n = 1
+        for v in dims:
+            self.n *= v

@@ -291,6 +291,12 @@ struct mpfft_mp_plan {
   unsigned long n_real = 0;
   // points per signal the staging buffers hold (the half spectrum of a real plan has N+1)
   unsigned long pts_max() const { return real ? N + 1 : N; }
+  // multi-dimensional plan: dims[0] x ... x dims[rank-1] = N points, row-major
+  int rank = 1;
+  unsigned long dims[3] = {0, 0, 0};
+  std::unique_ptr<mpfft_mp_plan> axis[3];  // rank > 1: one-dimensional plan of each axis (same L)
+  uint32_t *d_tmp = nullptr;               // rank > 1: transposition buffer, grown on demand
+  size_t tmp_words = 0;
   uint32_t *d_big = nullptr;  // streaming-kernel scratch (L > kMaxLimbs), grown on demand
   size_t big_words = 0;
   DeviceTree tree;
@@ -313,6 +319,7 @@ struct mpfft_mp_plan {
     int64_t *h_ei = nullptr, *d_ei = nullptr, *h_eo = nullptr, *d_eo = nullptr, *d_es = nullptr;
     uint8_t *h_si = nullptr, *d_si = nullptr, *h_so = nullptr, *d_so = nullptr;
     uint32_t *d_big = nullptr;  // streaming-kernel scratch of this slot (L > kMaxLimbs)
+    uint32_t *d_tmp = nullptr;  // transposition buffer of this slot (multi-dimensional plans)
   };
   ConvSlot cv[2];
   unsigned long cv_chunk = 0;  // signals per chunk the slots hold
@@ -320,7 +327,8 @@ struct mpfft_mp_plan {
   void free_conv() {
     for (auto &c : cv) {
       for (void *q : {(void *)c.d_in, (void *)c.d_out, (void *)c.d_mi, (void *)c.d_mo, (void *)c.d_ei,
-                      (void *)c.d_eo, (void *)c.d_es, (void *)c.d_si, (void *)c.d_so, (void *)c.d_big})
+                      (void *)c.d_eo, (void *)c.d_es, (void *)c.d_si, (void *)c.d_so, (void *)c.d_big,
+                      (void *)c.d_tmp})
         if (q) cudaFree(q);
       for (void *q : {(void *)c.h_mi, (void *)c.h_mo, (void *)c.h_ei, (void *)c.h_eo, (void *)c.h_si, (void *)c.h_so})
         if (q) cudaFreeHost(q);
@@ -332,6 +340,7 @@ struct mpfft_mp_plan {
   }
   ~mpfft_mp_plan() {
     free_conv();
+    if (d_tmp) cudaFree(d_tmp);
     if (d_big) cudaFree(d_big);
     if (d_in) cudaFree(d_in);
     if (d_out) cudaFree(d_out);
@@ -343,6 +352,12 @@ struct mpfft_mp_plan {
 
 struct mpfft_d_plan {
   unsigned long N = 0;
+  // multi-dimensional plan: dims[0] x ... x dims[rank-1] = N points, row-major
+  int rank = 1;
+  unsigned long dims[3] = {0, 0, 0};
+  std::unique_ptr<mpfft_d_plan> axis[3];
+  double *d_tmp = nullptr;  // rank > 1: transposition buffer, grown on demand
+  size_t tmp_cap = 0;
   DeviceTree upper;                   // levels above the shared-memory sub-transforms
   std::vector<void *> dev_allocs;     // roots, perms, sub-schedule tables
   double *d_wr = nullptr, *d_wi = nullptr;
@@ -359,6 +374,7 @@ struct mpfft_d_plan {
     if (d_out) cudaFree(d_out);
     if (h_in) cudaFreeHost(h_in);
     if (h_out) cudaFreeHost(h_out);
+    if (d_tmp) cudaFree(d_tmp);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -375,12 +391,15 @@ static int device_ready() {
 
 // real: n real points, planned as an n/2-point complex transform whose limb
 // format (L, F) and twiddle table are those of an n-point transform.
-static int mp_plan_init(mpfft_mp_plan *p, unsigned long n, long prec, bool host_only = false, bool real = false) {
+// force_L > 0: use that limb count (the axes of a multi-dimensional plan take the
+// format of the whole signal)
+static int mp_plan_init(mpfft_mp_plan *p, unsigned long n, long prec, bool host_only = false, bool real = false,
+                        int force_L = 0) {
   if (!is_pow2(n)) return set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
   if (real && n < 2) return set_err(MPFFT_EINVAL, "a real transform needs n >= 2 (n=%lu)", n);
   if (prec < 2) return set_err(MPFFT_EINVAL, "precision %ld < 2", prec);
   if (n > (1UL << 26)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
-  int L = mp_limbs_for(n, prec);
+  int L = force_L > 0 ? force_L : mp_limbs_for(n, prec);
   if (L > kMaxLimbsBig)
     return set_err(MPFFT_EUNSUPPORTED, "precision %ld at n=%lu needs %d limbs (> %d supported)", prec, n, L,
                    kMaxLimbsBig);
@@ -403,6 +422,34 @@ static int mp_plan_init(mpfft_mp_plan *p, unsigned long n, long prec, bool host_
   p->tabs.tw = p->tw.d_tw;
   p->tabs.dneg = p->tw.d_dneg;
   p->tabs.tws = real ? 2 : 1;
+  CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  return MPFFT_OK;
+}
+
+// Multi-dimensional plan (rank 1..3, row-major, last index fastest): the limb
+// format of the whole N = prod(dims)-point signal, plus a one-dimensional
+// plan per axis with that format.
+static int mp_plan_init_nd(mpfft_mp_plan *p, int rank, const unsigned long *dims, long prec, bool host_only) {
+  if (rank < 1 || rank > 3 || !dims) return set_err(MPFFT_EINVAL, "rank must be 1, 2 or 3");
+  unsigned long n = 1;
+  for (int i = 0; i < rank; ++i) {
+    if (!is_pow2(dims[i])) return set_err(MPFFT_EINVAL, "dims[%d]=%lu is not a power of two", i, dims[i]);
+    if (dims[i] > (1UL << 26) || n > (1UL << 26) / dims[i])
+      return set_err(MPFFT_EUNSUPPORTED, "more than 2^26 points in total");
+    n *= dims[i];
+  }
+  if (rank == 1) return mp_plan_init(p, n, prec, host_only);
+  if (int e = mp_plan_init(p, n, prec, true)) return e;  // the format of the whole signal
+  p->host_only = host_only;
+  p->rank = rank;
+  for (int i = 0; i < rank; ++i) p->dims[i] = dims[i];
+  if (host_only) return MPFFT_OK;
+  if (int e = device_ready()) return e;
+  for (int i = 0; i < rank; ++i) {
+    p->axis[i].reset(new (std::nothrow) mpfft_mp_plan);
+    if (!p->axis[i]) return set_err(MPFFT_ENOMEM, "out of host memory");
+    if (int e = mp_plan_init(p->axis[i].get(), dims[i], prec, false, false, p->L)) return e;
+  }
   CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   return MPFFT_OK;
 }
@@ -523,6 +570,37 @@ static void mp_fill_nan(mpfr_t *a, unsigned long n) {
   for (unsigned long k = 0; k < n; ++k) mpfr_set_nan(a[k]);
 }
 
+// streaming/tensor-kernel scratch words of one transform of B signals (0 when unused)
+static size_t mp_plan_big_words(const mpfft_mp_plan *p, unsigned long B) {
+  if (p->L <= kMaxLimbs) return 0;
+  if (p->rank == 1) return mp_big_scratch_words(p->tabs, p->L, (int)B);
+  size_t w = 0;
+  for (int s = 0; s < p->rank; ++s)
+    w = std::max(w, mp_big_scratch_words(p->axis[s]->tabs, p->L, (int)(B * (p->N / p->dims[s]))));
+  return w;
+}
+
+// The plan's complex transform on device limb planes, any rank.  Rank > 1:
+// per axis, last first: rotate that axis to the front (transposition of
+// [N/d][d] elements of B words per limb plane, into tmp), then a batched
+// one-dimensional transform of length d over the other N/d points x B
+// signals (tmp -> out).  After the last round the planes are in natural
+// order again.  tmp: 2*L*N*B words.
+static cudaError_t mp_transform(const mpfft_mp_plan *p, const uint32_t *in, uint32_t *out, int B, cudaStream_t st,
+                                uint32_t *big, uint32_t *tmp, float *launch_ms = nullptr) {
+  if (p->rank == 1) return mp_run_transform(p->L, p->tabs, in, out, B, st, launch_ms, big);
+  const uint32_t *src = in;
+  for (int s = p->rank - 1; s >= 0; --s) {
+    const long long d = (long long)p->dims[s], R = (long long)p->N / d;
+    cudaError_t e = transpose_launch(src, tmp, 2LL * p->L, R, d, B, st);
+    if (e != cudaSuccess) return e;
+    if ((e = mp_run_transform(p->L, p->axis[s]->tabs, tmp, out, (int)(B * R), st, nullptr, big)) != cudaSuccess)
+      return e;
+    src = out;
+  }
+  return cudaSuccess;
+}
+
 static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int nlo) {
   if (chunk <= p->cv_chunk && nli <= p->cv_nli && nlo <= p->cv_nlo) return MPFFT_OK;
   p->free_conv();
@@ -549,7 +627,8 @@ static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int n
     dm((void **)&c.d_so, comp);
     hm((void **)&c.h_so, comp);
     dm((void **)&c.d_es, chunk * 8);
-    if (p->L > kMaxLimbs) dm((void **)&c.d_big, mp_big_scratch_words(p->tabs, p->L, (int)chunk) * 4);
+    if (p->L > kMaxLimbs) dm((void **)&c.d_big, mp_plan_big_words(p, chunk) * 4);
+    if (p->rank > 1) dm((void **)&c.d_tmp, words * 4);
   }
   if (!ok) {
     cudaGetLastError();
@@ -569,11 +648,11 @@ static inline int nlimbs64(long prec) { return (int)((prec + 63) / 64); }
 // a -> b, split b -> a (half spectrum, value 2X).  C2R: split a -> b (2Z with
 // planes exchanged), transform b -> a (planes exchanged: the inverse).
 static cudaError_t mp_device_pipeline(const mpfft_mp_plan *p, int mode, uint32_t *a, uint32_t *b, int B,
-                                      cudaStream_t st, uint32_t *big, uint32_t **res) {
+                                      cudaStream_t st, uint32_t *big, uint32_t *tmp, uint32_t **res) {
   cudaError_t e = cudaSuccess;
   if (mode == kComplex) {
     *res = b;
-    return mp_run_transform(p->L, p->tabs, a, b, B, st, nullptr, big);
+    return mp_transform(p, a, b, B, st, big, tmp);
   }
   *res = a;
   if (mode == kR2C) {
@@ -612,6 +691,7 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
   // butterfly), and at most ~256 MiB of staging per slot
   const size_t per_signal = (size_t)2 * p->pts_max() * ((nli + nlo) * 8 + 2 * 4 * p->L + 18);
   unsigned long chunk = std::min<unsigned long>(256, std::max<size_t>(32, (256UL << 20) / per_signal));
+  chunk = std::min<unsigned long>(chunk, (unsigned long)INT32_MAX / p->pts_max());  // batch x points fits an int
   if (chunk >= 32) chunk &= ~31UL;
   chunk = std::min(chunk, batch);
   if (int e = mp_conv_reserve(p, chunk, nli, nlo)) return e;
@@ -650,7 +730,7 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
     CUDA_TRY(cudaMemcpyAsync(c.d_si, c.h_si, ci_n, cudaMemcpyHostToDevice, c.st));
     CUDA_TRY(mp_import_launch(c.d_mi, c.d_ei, c.d_si, nli, (int)Ni, (int)cb, p->L, p->F, c.d_es, c.d_in, c.st));
     uint32_t *res = nullptr;
-    CUDA_TRY(mp_device_pipeline(p, mode, c.d_in, c.d_out, (int)cb, c.st, c.d_big, &res));
+    CUDA_TRY(mp_device_pipeline(p, mode, c.d_in, c.d_out, (int)cb, c.st, c.d_big, c.d_tmp, &res));
     CUDA_TRY(mp_export_launch(res, (int)No, (int)cb, p->L, c.d_es, p->F + fadj, prec_out, nlo, c.d_mo, c.d_eo,
                               c.d_so, c.st));
     CUDA_TRY(cudaMemcpyAsync(c.h_mo, c.d_mo, co_n * nlo * 8, cudaMemcpyDeviceToHost, c.st));
@@ -712,7 +792,7 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
 static int mp_big_reserve(mpfft_mp_plan *p, unsigned long batch, uint32_t **out) {
   *out = nullptr;
   if (p->L <= kMaxLimbs) return MPFFT_OK;
-  const size_t words = mp_big_scratch_words(p->tabs, p->L, (int)batch);
+  const size_t words = mp_plan_big_words(p, batch);
   if (words > p->big_words) {
     if (p->d_big) cudaFree(p->d_big);
     p->d_big = nullptr;
@@ -727,9 +807,29 @@ static int mp_big_reserve(mpfft_mp_plan *p, unsigned long batch, uint32_t **out)
   return MPFFT_OK;
 }
 
+// transposition buffer of a multi-dimensional plan for a batch; null for rank 1
+static int mp_tmp_reserve(mpfft_mp_plan *p, unsigned long batch, uint32_t **out) {
+  *out = nullptr;
+  if (p->rank == 1) return MPFFT_OK;
+  const size_t words = (size_t)2 * p->L * p->N * batch;
+  if (words > p->tmp_words) {
+    if (p->d_tmp) cudaFree(p->d_tmp);
+    p->d_tmp = nullptr;
+    p->tmp_words = 0;
+    if (cudaMalloc(&p->d_tmp, words * 4) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(MPFFT_ENOMEM, "cannot allocate %zu bytes of transposition scratch", words * 4);
+    }
+    p->tmp_words = words;
+  }
+  *out = p->d_tmp;
+  return MPFFT_OK;
+}
+
 // after a synchronous execution: a tensor-core wait that expired voids the results
 static int mp_tc_check(const mpfft_mp_plan *p, int rc) {
-  if (rc != MPFFT_OK || !mp_tc_used(p->tabs, p->L)) return rc;
+  const MpDeviceTables &T = p->rank > 1 ? p->axis[0]->tabs : p->tabs;
+  if (rc != MPFFT_OK || !mp_tc_used(T, p->L)) return rc;
   int code = 0;
   CUDA_TRY(mp_tc_take_error(&code));
   if (code) return set_err(MPFFT_ECUDA, "a tensor-core wait expired (code %d)", code);
@@ -744,15 +844,18 @@ static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, int mode, cons
     const int r = mp_execute_gpuconv(p, batch, mode, ii, inr, ini, oo, outr, outi, fadj);
     if (r != -1) return mp_tc_check(p, r);
   }
+  if ((unsigned long long)batch * p->pts_max() > (unsigned long long)INT32_MAX)
+    return set_err(MPFFT_EUNSUPPORTED, "batch too large for host conversion");
   if (int e = mp_reserve(p, batch)) return e;
   p->exps.assign(batch, 0);
   if (int e = mp_pack_impl(p, batch, ii, inr, ini, p->h_in, p->exps.data())) return e;
-  uint32_t *big = nullptr;
+  uint32_t *big = nullptr, *tmp = nullptr;
   if (int e = mp_big_reserve(p, batch, &big)) return e;
+  if (int e = mp_tmp_reserve(p, batch, &tmp)) return e;
   uint32_t *res = nullptr;
   CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, (size_t)2 * p->L * ii.n * batch * 4, cudaMemcpyHostToDevice,
                            p->stream));
-  CUDA_TRY(mp_device_pipeline(p, mode, p->d_in, p->d_out, (int)batch, p->stream, big, &res));
+  CUDA_TRY(mp_device_pipeline(p, mode, p->d_in, p->d_out, (int)batch, p->stream, big, tmp, &res));
   CUDA_TRY(cudaMemcpyAsync(p->h_out, res, (size_t)2 * p->L * oo.n * batch * 4, cudaMemcpyDeviceToHost, p->stream));
   CUDA_TRY(cudaStreamSynchronize(p->stream));
   if (int e = mp_tc_check(p, MPFFT_OK)) return e;
@@ -925,10 +1028,80 @@ static double d_scale(const mpfft_d_plan *p, unsigned flags) {
   return (flags & MPFFT_SCALED) ? 1.0 / (double)p->N : 1.0;
 }
 
+static int d_plan_init_nd(mpfft_d_plan *p, int rank, const unsigned long *dims) {
+  if (rank < 1 || rank > 3 || !dims) return set_err(MPFFT_EINVAL, "rank must be 1, 2 or 3");
+  unsigned long n = 1;
+  for (int i = 0; i < rank; ++i) {
+    if (!is_pow2(dims[i])) return set_err(MPFFT_EINVAL, "dims[%d]=%lu is not a power of two", i, dims[i]);
+    if (dims[i] > (1UL << 28) || n > (1UL << 28) / dims[i])
+      return set_err(MPFFT_EUNSUPPORTED, "more than 2^28 points in total");
+    n *= dims[i];
+  }
+  if (rank == 1) return d_plan_init(p, n);
+  if (int e = device_ready()) return e;
+  p->N = n;
+  p->rank = rank;
+  for (int i = 0; i < rank; ++i) {
+    p->dims[i] = dims[i];
+    p->axis[i].reset(new (std::nothrow) mpfft_d_plan);
+    if (!p->axis[i]) return set_err(MPFFT_ENOMEM, "out of host memory");
+    if (int e = d_plan_init(p->axis[i].get(), dims[i])) return e;
+  }
+  CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  return MPFFT_OK;
+}
+
+// The plan's transform in the FP64 layout [c][b][p], any rank.  Rank > 1: per
+// axis, last first: a batched one-dimensional transform along the innermost
+// axis (in -> tmp; the other points are more signals), then a transposition
+// of each component of each signal, [N/d][d] -> [d][N/d] (tmp -> out), which
+// brings the next axis innermost; after the last round the points are in
+// natural order again.  Every one-dimensional transform is the reference's
+// (bit-identical), so the result equals the axis-by-axis application of
+// d_sr24_cp_fft in this order.  Scaling by 1/d per axis is exact.
+static cudaError_t d_transform(mpfft_d_plan *p, const double *in, double *out, int B, unsigned flags,
+                               cudaStream_t st, double *tmp) {
+  if (p->rank == 1) return d_run_transform(p->tabs, in, out, B, d_scale(p, flags), st);
+  const double *src = in;
+  for (int s = p->rank - 1; s >= 0; --s) {
+    const long long d = (long long)p->dims[s], R = (long long)p->N / d;
+    const double sc = (flags & MPFFT_SCALED) ? 1.0 / (double)d : 1.0;
+    cudaError_t e = d_run_transform(p->axis[s]->tabs, src, tmp, (int)(B * R), sc, st);
+    if (e != cudaSuccess) return e;
+    e = transpose_launch(reinterpret_cast<const uint32_t *>(tmp), reinterpret_cast<uint32_t *>(out), 2LL * B, R, d, 2,
+                         st);
+    if (e != cudaSuccess) return e;
+    src = out;
+  }
+  return cudaSuccess;
+}
+
+static int d_tmp_reserve(mpfft_d_plan *p, unsigned long batch, double **out) {
+  *out = nullptr;
+  if (p->rank == 1) return MPFFT_OK;
+  const size_t words = (size_t)2 * p->N * batch;
+  if (words > p->tmp_cap) {
+    if (p->d_tmp) cudaFree(p->d_tmp);
+    p->d_tmp = nullptr;
+    p->tmp_cap = 0;
+    if (cudaMalloc(&p->d_tmp, words * 8) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(MPFFT_ENOMEM, "cannot allocate %zu bytes of transposition scratch", words * 8);
+    }
+    p->tmp_cap = words;
+  }
+  *out = p->d_tmp;
+  return MPFFT_OK;
+}
+
 static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *inr, const double *ini,
                           unsigned long s, double *outr, double *outi, unsigned flags) {
   std::lock_guard<std::mutex> g(p->mu);
+  if ((unsigned long long)batch * p->N > (unsigned long long)INT32_MAX)
+    return set_err(MPFFT_EUNSUPPORTED, "batch too large");
   if (int e = d_reserve(p, batch)) return e;
+  double *tmp = nullptr;
+  if (int e = d_tmp_reserve(p, batch, &tmp)) return e;
   const unsigned long N = p->N;
   const size_t cim = (size_t)N * batch;
   // [c][b][p]: each signal contiguous
@@ -943,7 +1116,7 @@ static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *in
   }
   const size_t bytes = 2 * cim * sizeof(double);
   CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, bytes, cudaMemcpyHostToDevice, p->stream));
-  CUDA_TRY(d_run_transform(p->tabs, p->d_in, p->d_out, (int)batch, d_scale(p, flags), p->stream));
+  CUDA_TRY(d_transform(p, p->d_in, p->d_out, (int)batch, flags, p->stream, tmp));
   CUDA_TRY(cudaMemcpyAsync(p->h_out, p->d_out, bytes, cudaMemcpyDeviceToHost, p->stream));
   CUDA_TRY(cudaStreamSynchronize(p->stream));
   memcpy(outr, p->h_out, cim * sizeof(double));
@@ -1052,6 +1225,23 @@ MPFFT_API int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, 
   return set_err(MPFFT_OK, "");
 }
 
+MPFFT_API int mpfft_mp_plan_create_nd(mpfft_mp_plan **plan, int rank, const unsigned long *dims, long prec,
+                                      unsigned flags) {
+  if (!plan) return set_err(MPFFT_EINVAL, "NULL plan pointer");
+  *plan = nullptr;
+  std::unique_ptr<mpfft_mp_plan> p(new (std::nothrow) mpfft_mp_plan);
+  if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
+  if (int e = mp_plan_init_nd(p.get(), rank, dims, prec, (flags & MPFFT_PLAN_HOST_ONLY) != 0)) return e;
+  p->force_host_conversion = (flags & MPFFT_PLAN_HOST_CONVERSION) != 0;
+  if (flags & MPFFT_PLAN_NO_TENSOR) {
+    p->tabs.tc = 0;
+    for (auto &a : p->axis)
+      if (a) a->tabs.tc = 0;
+  }
+  *plan = p.release();
+  return set_err(MPFFT_OK, "");
+}
+
 MPFFT_API int mpfft_mp_plan_create(mpfft_mp_plan **plan, unsigned long n, long prec) {
   return mpfft_mp_plan_create_flags(plan, n, prec, 0);
 }
@@ -1135,10 +1325,12 @@ MPFFT_API int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, 
   const size_t bytes = (size_t)2 * plan->L * plan->N * batch * 4;
   const char *a = (const char *)d_in, *b = (const char *)d_out;
   if (a < b + bytes && b < a + bytes) return set_err(MPFFT_EINVAL, "input and output buffers overlap");
-  if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");
-  uint32_t *big = nullptr;
+  if (batch > (unsigned long)INT32_MAX || (unsigned long long)batch * plan->N > (unsigned long long)INT32_MAX)
+    return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  uint32_t *big = nullptr, *tmp = nullptr;
   if (int e = mp_big_reserve(plan, batch, &big)) return e;
-  CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream, nullptr, big));
+  if (int e = mp_tmp_reserve(plan, batch, &tmp)) return e;
+  CUDA_TRY(mp_transform(plan, d_in, d_out, (int)batch, (cudaStream_t)stream, big, tmp));
   return set_err(MPFFT_OK, "");
 }
 
@@ -1169,6 +1361,16 @@ MPFFT_API int mpfft_d_plan_create(mpfft_d_plan **plan, unsigned long n) {
   return set_err(MPFFT_OK, "");
 }
 
+MPFFT_API int mpfft_d_plan_create_nd(mpfft_d_plan **plan, int rank, const unsigned long *dims) {
+  if (!plan) return set_err(MPFFT_EINVAL, "NULL plan pointer");
+  *plan = nullptr;
+  std::unique_ptr<mpfft_d_plan> p(new (std::nothrow) mpfft_d_plan);
+  if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
+  if (int e = d_plan_init_nd(p.get(), rank, dims)) return e;
+  *plan = p.release();
+  return set_err(MPFFT_OK, "");
+}
+
 MPFFT_API int mpfft_d_plan_destroy(mpfft_d_plan *plan) {
   delete plan;
   return set_err(MPFFT_OK, "");
@@ -1193,7 +1395,14 @@ MPFFT_API int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, co
   const size_t bytes = (size_t)2 * plan->N * batch * 8;
   const char *a = (const char *)d_in, *b = (const char *)d_out;
   if (a < b + bytes && b < a + bytes) return set_err(MPFFT_EINVAL, "input and output buffers overlap");
-  CUDA_TRY(d_run_transform(plan->tabs, d_in, d_out, (int)batch, d_scale(plan, flags), (cudaStream_t)stream));
+  if ((unsigned long long)batch * plan->N > (unsigned long long)INT32_MAX)
+    return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  double *tmp = nullptr;
+  {
+    std::lock_guard<std::mutex> g(plan->mu);
+    if (int e = d_tmp_reserve(plan, batch, &tmp)) return e;
+  }
+  CUDA_TRY(d_transform(plan, d_in, d_out, (int)batch, flags, (cudaStream_t)stream, tmp));
   return set_err(MPFFT_OK, "");
 }
 
@@ -1202,7 +1411,7 @@ MPFFT_API int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, co
 // ---------------------------------------------------------------------------
 
 MPFFT_API int mpfft_mp_plan_schedule(const mpfft_mp_plan *plan, int *level_n, int *level_nodes, int max_levels) {
-  if (!plan || plan->host_only) return -1;
+  if (!plan || plan->host_only || plan->rank > 1) return -1;
   const int n = plan->tabs.nlevels;
   for (int i = 0; i < n && i < max_levels; ++i) {
     level_n[i] = plan->tabs.level_n[i];
@@ -1216,6 +1425,7 @@ MPFFT_API int mpfft_mp_execute_device_timed(mpfft_mp_plan *plan, unsigned long b
   if (!plan || !d_in || !d_out || !launch_ms) return set_err(MPFFT_EINVAL, "NULL argument");
   if (plan->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
   if (plan->real) return set_err(MPFFT_EINVAL, "real plans have no device-layout entry point");
+  if (plan->rank > 1) return set_err(MPFFT_EINVAL, "per-launch timing is for one-dimensional plans");
   uint32_t *big = nullptr;
   if (int e = mp_big_reserve(plan, batch, &big)) return e;
   CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream, launch_ms, big));
@@ -1260,6 +1470,7 @@ MPFFT_API int mpfft_mp_execute_significands_static(const mpfft_mp_plan *plan, un
     return set_err(MPFFT_EINVAL, "NULL argument");
   if (plan->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
   if (plan->real) return set_err(MPFFT_EINVAL, "real plans have no device-layout entry point");
+  if (plan->rank > 1) return set_err(MPFFT_EINVAL, "the static-scratch entry point takes one-dimensional plans");
   if (nl_in < 1 || prec_out < 2) return set_err(MPFFT_EINVAL, "nl_in must be >= 1 and prec_out >= 2");
   if (batch == 0) return set_err(MPFFT_OK, "");
   if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");

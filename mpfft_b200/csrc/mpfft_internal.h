@@ -166,6 +166,9 @@ cudaError_t mp_import_launch(const uint64_t *mant, const int64_t *ex, const uint
                              int L, long F, int64_t *es, uint32_t *planes, cudaStream_t s);
 cudaError_t mp_export_launch(const uint32_t *planes, int N, int B, int L, const int64_t *es, long F_plus_shift,
                              long prec, int nlo, uint64_t *out, int64_t *oex, uint8_t *osg, cudaStream_t s);
+// out[m][c][r][e] = in[m][r][c][e]: nmat matrices of R x C elements of E words
+cudaError_t transpose_launch(const uint32_t *in, uint32_t *out, long long nmat, long long R, long long C, int E,
+                             cudaStream_t s);
 // FP64 layout: word (c, b, p) at base[(c*B + b)*N + p]  (signal-contiguous)
 cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
                             cudaStream_t s);

@@ -436,6 +436,44 @@ OAPI void orc_mp_dft(unsigned long N, long prec, mpfr_t *xr, mpfr_t *xi, mpfr_t 
   orc_mp_free(sw, N);
 }
 
+/* Multi-dimensional DFT of rank dimensions dims[0] x ... (row-major, last
+ * index fastest) at precision prec: the direct DFT above along every axis in
+ * turn, each line rounded into prec-bit intermediates. */
+OAPI void orc_mp_dft_nd(int rank, const unsigned long *dims, long prec, mpfr_t *xr, mpfr_t *xi, mpfr_t *yr,
+                        mpfr_t *yi) {
+  unsigned long n = 1;
+  for (int a = 0; a < rank; a++) n *= dims[a];
+  for (unsigned long k = 0; k < n; k++) {
+    mpfr_set(yr[k], xr[k], RN);
+    mpfr_set(yi[k], xi[k], RN);
+  }
+  unsigned long stride = n;
+  for (int a = 0; a < rank; a++) {
+    const unsigned long d = dims[a];
+    stride /= d;  /* distance between consecutive points of axis a */
+    const unsigned long outer = n / (d * stride);
+    mpfr_t *lr = orc_mp_alloc(d, prec), *li = orc_mp_alloc(d, prec);
+    mpfr_t *tr = orc_mp_alloc(d, prec), *ti = orc_mp_alloc(d, prec);
+    for (unsigned long o = 0; o < outer; o++)
+      for (unsigned long q = 0; q < stride; q++) {
+        const unsigned long base = o * d * stride + q;
+        for (unsigned long j = 0; j < d; j++) {
+          mpfr_set(lr[j], yr[base + j * stride], RN);
+          mpfr_set(li[j], yi[base + j * stride], RN);
+        }
+        orc_mp_dft(d, prec, lr, li, tr, ti);
+        for (unsigned long j = 0; j < d; j++) {
+          mpfr_set(yr[base + j * stride], tr[j], RN);
+          mpfr_set(yi[base + j * stride], ti[j], RN);
+        }
+      }
+    orc_mp_free(lr, d);
+    orc_mp_free(li, d);
+    orc_mp_free(tr, d);
+    orc_mp_free(ti, d);
+  }
+}
+
 /* ------------------------------------------------------------------------ */
 /* error metrics                                                            */
 /* ------------------------------------------------------------------------ */

@@ -69,6 +69,7 @@ def lib() -> C.CDLL:
         "orc_mp_fft_top": (None, [vp, vp, vp, vp, vp]),
         "orc_mp_dft": (None, [ul, sl, vp, vp, vp, vp]),
         "orc_mp_hermitian_extend": (None, [ul, vp, vp, vp, vp]),
+        "orc_mp_dft_nd": (None, [C.c_int, C.POINTER(C.c_ulong), sl, vp, vp, vp, vp]),
         "orc_mp_errors": (None, [ul, vp, vp, vp, vp, dp]),
         "orc_d_new": (vp, [ul]),
         "orc_d_delete": (None, [vp]),
@@ -174,6 +175,12 @@ class MpFFT:
 def mp_dft(xr, xi, yr, yi) -> None:
     """Direct DFT at the output arrays' precision (prec of yr[0])."""
     lib().orc_mp_dft(xr.n, yr.prec, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
+
+
+def mp_dft_nd(dims, xr, xi, yr, yi) -> None:
+    """Row-major multi-dimensional DFT at the output arrays' precision."""
+    d = (C.c_ulong * len(dims))(*dims)
+    lib().orc_mp_dft_nd(len(dims), d, yr.prec, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
 
 
 def mp_errors(yr, yi, rr, ri) -> dict:

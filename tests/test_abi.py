@@ -148,3 +148,24 @@ def test_real_plan_argument_validation(M):
     with pytest.raises(M.MpfftError) as e:
         M.MpRealPlan(1024, 2048)  # 66 limbs: beyond the 34-limb register kernels
     assert e.value.code == M.EUNSUPPORTED
+
+
+def test_nd_plan_argument_validation(M):
+    """Rank 1..3, power-of-two dims, at most 2^26 points (mp); checked before
+    any device work (a host-only mp plan needs no GPU)."""
+    import ctypes as C
+
+    pl = M.MpPlanND((16, 32), 256, host_only=True)
+    lg = 9
+    assert pl.n == 512 and pl.frac_bits == 32 * pl.limbs - 1 - (lg + 2)
+    for dims in ((), (2, 2, 2, 2), (12, 4), (4, 0)):
+        with pytest.raises(M.MpfftError) as e:
+            M.MpPlanND(dims, 64, host_only=True)
+        assert e.value.code == M.EINVAL
+    with pytest.raises(M.MpfftError) as e:
+        M.MpPlanND((1 << 14, 1 << 13), 64, host_only=True)
+    assert e.value.code == M.EUNSUPPORTED
+    for dims in ((3, 4), (4, 4, 4, 4)):
+        d = (C.c_ulong * len(dims))(*dims)
+        h = C.c_void_p()
+        assert M.lib.mpfft_d_plan_create_nd(C.byref(h), len(dims), d) == M.EINVAL
