@@ -223,10 +223,10 @@ __device__ __forceinline__ void d_butterfly_smem(double *yr, double *yi, int off
 // the big schedule.  Otherwise G = 1 and the CTA's root may be of size T or
 // T/2.  Per instance: gather the root's input sequence in input order
 // (coalesced reads) into DIT positions, leaves, levels, then write the outputs
-// once.  The twiddles the levels need, LUT[m*(N/T)] for m < T/4, are staged in
-// shared memory once per CTA.
+// once.  The twiddles the levels need, LUT[m*(N/T)] for m < T/4, are read
+// through L1 (a few KB, shared by all CTAs).
 template <bool SINGLE>
-__global__ void __launch_bounds__(256, 2) d_sub_kernel(const double *__restrict__ in, double *__restrict__ out, int N,
+__global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict__ in, double *__restrict__ out, int N,
                                                         int B, const SubRoot *__restrict__ roots, int nroots, int G,
                                                         SubSchedule big, SubSchedule small,
                                                         const double *__restrict__ wr, const double *__restrict__ wi,
@@ -235,11 +235,7 @@ __global__ void __launch_bounds__(256, 2) d_sub_kernel(const double *__restrict_
   const int Tmax = big.size;
   const int lgT = 31 - __clz(Tmax);
   const int istride = 2 * (pidx(Tmax) + 1);  // doubles per instance
-  double *twr = sm + (size_t)G * istride, *twi = twr + Tmax / 4 + 1;
-  for (int m = threadIdx.x; m < Tmax / 4; m += blockDim.x) {
-    twr[m] = wr[(size_t)m * (N / Tmax)];
-    twi[m] = wi[(size_t)m * (N / Tmax)];
-  }
+  const int tws = N / Tmax;                  // twiddle table stride of this sub-transform
   // this CTA's instances
   int G_here, b0;
   SubRoot rt;
@@ -261,17 +257,32 @@ __global__ void __launch_bounds__(256, 2) d_sub_kernel(const double *__restrict_
   const int nleaves = is_big ? big.nleaves : small.nleaves;
   const int n16 = is_big ? big.nleaf16 : small.nleaf16, n8 = is_big ? big.nleaf8 : small.nleaf8;
   const int nlevels = is_big ? big.nlevels : small.nlevels;
-  // gather: element j of instance g to DIT position perm[j]
-  for (int e = threadIdx.x; e < (G_here << lgT); e += blockDim.x) {
-    const int g = e >> lgT, j = e & (Tmax - 1);
-    if (!SINGLE && j >= T) continue;
-    int idx = rt.sn + j * rt.s;
-    if (idx < 0) idx += N;
-    const int b = b0 + g;
-    double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
-    const int m = perm[j];
-    yr[pidx(m)] = in[(size_t)b * N + idx];
-    yi[pidx(m)] = in[((size_t)B + b) * N + idx];
+  // gather: element j of instance g to DIT position perm[j]; 8 elements per
+  // thread are loaded before any is stored, so their latencies overlap
+  const int total = G_here << lgT;
+  for (int e0 = 0; e0 < total; e0 += 8 * 256) {
+    double vr[8], vi[8];
+    int dst[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * 256 + (int)threadIdx.x;
+      const int g = e >> lgT, j = e & (Tmax - 1);
+      dst[u] = -1;
+      if (e < total && (SINGLE || j < T)) {
+        int idx = rt.sn + j * rt.s;
+        if (idx < 0) idx += N;
+        const size_t b = (size_t)(b0 + g);
+        vr[u] = in[b * N + idx];
+        vi[u] = in[((size_t)B + b) * N + idx];
+        dst[u] = g * istride + pidx(perm[j]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (dst[u] >= 0) {
+        sm[dst[u]] = vr[u];
+        sm[dst[u] + pidx(Tmax) + 1] = vi[u];
+      }
   }
   __syncthreads();
   // leaves, grouped by size: 16-point, then 8-point, then (N <= 4 only) smaller
@@ -305,7 +316,7 @@ __global__ void __launch_bounds__(256, 2) d_sub_kernel(const double *__restrict_
       const int node = t >> lgq, k = t & (q - 1);
       const int km = k << (lgT - (lgq + 2));  // k * (T/n)
       double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
-      d_butterfly_smem(yr, yi, nodes[node], k, q, twr[km], twi[km], sc);
+      d_butterfly_smem(yr, yi, nodes[node], k, q, __ldg(wr + (size_t)km * tws), __ldg(wi + (size_t)km * tws), sc);
     }
   }
   __syncthreads();
@@ -348,7 +359,7 @@ cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *ou
   const DConst K{T.c8, T.c16a, T.c16b, T.c16c, T.c16d};
   const int size = T.sub[0].size;
   const int G = d_sub_instances(T);
-  const size_t smem = ((size_t)G * 2 * (size + size / 16 + 1) + 2 * (size / 4 + 1)) * sizeof(double);
+  const size_t smem = ((size_t)G * 2 * (size + size / 16 + 1)) * sizeof(double);
   static bool attr_set = false;  // idempotent; benign race
   if (!attr_set) {
     cudaFuncSetAttribute(d_sub_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
