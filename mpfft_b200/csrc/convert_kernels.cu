@@ -37,18 +37,38 @@ __global__ void mp_import_exp_init(int64_t *es, int B) {
   if (b < B) es[b] = kZeroExp;
 }
 
+// Index of component (c, p, b) in the mant/ex/sg arrays: (c*N + p)*B + b
+// (batch innermost), or with sig_major (b*2 + c)*N + p (each signal's
+// components contiguous, the order a host walks mpfr_t arrays in).
+__device__ __forceinline__ size_t comp_index(bool sig_major, long long t, int b, int c, int p, int N) {
+  return sig_major ? ((size_t)b * 2 + c) * N + p : (size_t)t;
+}
+
 // block exponents: es[b] = max exp over signal b's nonzero components
-// component (c, p, b) at index (c*N + p)*B + b
-__global__ void mp_import_exp(const int64_t *__restrict__ ex, int N, int B, int64_t *__restrict__ es) {
+// (t runs over the storage index)
+// (t runs over the storage index).  Lanes of a warp that share a signal (all of
+// them in the signal-major layout) first reduce among themselves, so each
+// signal takes one atomic per warp.
+__global__ void mp_import_exp(const int64_t *__restrict__ ex, int N, int B, bool sig_major,
+                              int64_t *__restrict__ es) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 2LL * N * B) return;
-  const int64_t e = ex[t];
-  if (e != kZeroExp) atomicMax((long long *)&es[t % B], (long long)e);
+  const bool in = t < 2LL * N * B;
+  long long v = in ? (long long)ex[t] : (long long)kZeroExp;  // kZeroExp is the identity of max
+  const int b = in ? (sig_major ? (int)(t / (2LL * N)) : (int)(t % B)) : -1;
+  const int lane = threadIdx.x & 31;
+  for (int off = 1; off < 32; off <<= 1) {  // segmented max over the contiguous lanes of one signal
+    const long long ov = __shfl_down_sync(0xffffffffu, v, off);
+    const int ob = __shfl_down_sync(0xffffffffu, b, off);
+    if (lane + off < 32 && ob == b && ov > v) v = ov;
+  }
+  const int pb = __shfl_up_sync(0xffffffffu, b, 1);
+  const bool head = lane == 0 || pb != b;
+  if (in && head && v != (long long)kZeroExp) atomicMax((long long *)&es[b], v);
 }
 
 // mant: [component][nl] 64-bit limbs; planes: word (c, i, p, b) at ((c*L + i)*N + p)*B + b
 __global__ void mp_import(const uint64_t *__restrict__ mant, const int64_t *__restrict__ ex,
-                          const uint8_t *__restrict__ sg, int nl, int N, int B, int L, long F,
+                          const uint8_t *__restrict__ sg, int nl, int N, int B, int L, long F, bool sig_major,
                           const int64_t *__restrict__ es, uint32_t *__restrict__ planes) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 2LL * N * B) return;
@@ -58,12 +78,13 @@ __global__ void mp_import(const uint64_t *__restrict__ mant, const int64_t *__re
   const int p = (int)(cp - (long long)c * N);
   const size_t plane = (size_t)N * B;
   uint32_t *dst = planes + ((size_t)c * L * N + p) * B + b;
-  const int64_t e = ex[t];
+  const size_t ci = comp_index(sig_major, t, b, c, p, N);
+  const int64_t e = ex[ci];
   if (e == kZeroExp) {
     for (int i = 0; i < L; ++i) dst[(size_t)i * plane] = 0;
     return;
   }
-  const uint64_t *m = mant + (size_t)t * nl;
+  const uint64_t *m = mant + ci * nl;
   // value = M * 2^(e - 64 nl);  A = M * 2^sh
   const long sh = (long)(e - 64L * nl + F - es[b]);
   uint32_t round = 0;
@@ -71,7 +92,7 @@ __global__ void mp_import(const uint64_t *__restrict__ mant, const int64_t *__re
     const long rb = -sh - 1;
     round = rb < 64L * nl ? (bits32_64(m, nl, rb) & 1u) : 0u;
   }
-  const bool neg = sg[t] != 0;
+  const bool neg = sg[ci] != 0;
   uint32_t cr = round;           // rounding carry (magnitude)
   uint32_t cn = neg ? 1u : 0u;   // negation carry (two's complement)
   const uint32_t mk = neg ? 0xffffffffu : 0u;
@@ -86,7 +107,7 @@ __global__ void mp_import(const uint64_t *__restrict__ mant, const int64_t *__re
 
 // out: [component][nlo] 64-bit limbs, oex (kZeroExp for zero), osg
 __global__ void mp_export(const uint32_t *__restrict__ planes, int N, int B, int L, const int64_t *__restrict__ es,
-                          long F_plus_shift, long prec, int nlo, uint64_t *__restrict__ out,
+                          long F_plus_shift, long prec, int nlo, bool sig_major, uint64_t *__restrict__ out,
                           int64_t *__restrict__ oex, uint8_t *__restrict__ osg) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 2LL * N * B) return;
@@ -96,6 +117,7 @@ __global__ void mp_export(const uint32_t *__restrict__ planes, int N, int B, int
   const int p = (int)(cp - (long long)c * N);
   const size_t plane = (size_t)N * B;
   const uint32_t *src = planes + ((size_t)c * L * N + p) * B + b;
+  const size_t ci = comp_index(sig_major, t, b, c, p, N);
   uint64_t a[(kMaxLimbsBig + 2) / 2 + 1];  // magnitude in 64-bit limbs
   const int na = (L + 1) / 2;
   const bool neg = (src[(size_t)(L - 1) * plane] >> 31) != 0;
@@ -115,10 +137,10 @@ __global__ void mp_export(const uint32_t *__restrict__ planes, int N, int B, int
       top = 64 * i + 63 - __clzll((long long)a[i]);
       break;
     }
-  uint64_t *o = out + (size_t)t * nlo;
+  uint64_t *o = out + ci * nlo;
   if (top < 0) {
-    oex[t] = kZeroExp;
-    osg[t] = 0;
+    oex[ci] = kZeroExp;
+    osg[ci] = 0;
     for (int k = 0; k < nlo; ++k) o[k] = 0;
     return;
   }
@@ -167,25 +189,26 @@ __global__ void mp_export(const uint32_t *__restrict__ planes, int N, int B, int
     for (int k = 0; k < nlo - 1; ++k) o[k] = 0;
     e += 1;
   }
-  oex[t] = (int64_t)(e + (long)es[b] - F_plus_shift);
-  osg[t] = neg ? 1 : 0;
+  oex[ci] = (int64_t)(e + (long)es[b] - F_plus_shift);
+  osg[ci] = neg ? 1 : 0;
 }
 
 cudaError_t mp_import_launch(const uint64_t *mant, const int64_t *ex, const uint8_t *sg, int nl, int N, int B,
-                             int L, long F, int64_t *es, uint32_t *planes, cudaStream_t s) {
+                             int L, long F, int64_t *es, uint32_t *planes, cudaStream_t s, bool sig_major) {
   mp_import_exp_init<<<(B + 255) / 256, 256, 0, s>>>(es, B);
   const long long total = 2LL * N * B;
   const int blocks = (int)((total + 255) / 256);
-  mp_import_exp<<<blocks, 256, 0, s>>>(ex, N, B, es);
-  mp_import<<<blocks, 256, 0, s>>>(mant, ex, sg, nl, N, B, L, F, es, planes);
+  mp_import_exp<<<blocks, 256, 0, s>>>(ex, N, B, sig_major, es);
+  mp_import<<<blocks, 256, 0, s>>>(mant, ex, sg, nl, N, B, L, F, sig_major, es, planes);
   return cudaGetLastError();
 }
 
 cudaError_t mp_export_launch(const uint32_t *planes, int N, int B, int L, const int64_t *es, long F_plus_shift,
-                             long prec, int nlo, uint64_t *out, int64_t *oex, uint8_t *osg, cudaStream_t s) {
+                             long prec, int nlo, uint64_t *out, int64_t *oex, uint8_t *osg, cudaStream_t s,
+                             bool sig_major) {
   const long long total = 2LL * N * B;
   const int blocks = (int)((total + 255) / 256);
-  mp_export<<<blocks, 256, 0, s>>>(planes, N, B, L, es, F_plus_shift, prec, nlo, out, oex, osg);
+  mp_export<<<blocks, 256, 0, s>>>(planes, N, B, L, es, F_plus_shift, prec, nlo, sig_major, out, oex, osg);
   return cudaGetLastError();
 }
 

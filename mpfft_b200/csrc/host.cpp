@@ -23,8 +23,15 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <atomic>
+#include <condition_variable>
 #include <thread>
 #include <vector>
+
+#include <unistd.h>
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
 
 #include <cuda_runtime.h>
 
@@ -194,6 +201,89 @@ static void fixed_to_mpfr(const uint32_t *A, int L, long e2, mpfr_ptr y) {
   mpfr_set_z_2exp(y, &z, e2, MPFR_RNDN);
 }
 
+// A process-wide pool of hardware_concurrency - 1 workers for the host-side
+// conversion loops (they run several times per call on large batches, so
+// thread start-up would show).  One job at a time: a caller that finds the pool
+// busy, or runs in a process forked after the pool was started (whose workers
+// did not survive the fork), falls back to its own threads.
+class WorkerPool {
+ public:
+  static WorkerPool &get() {
+    static WorkerPool pool;
+    return pool;
+  }
+  // fn over parts [i*chunk, min(n, (i+1)*chunk)), i < nparts; false when unavailable
+  bool run(long n, long nparts, long chunk, const std::function<void(long, long)> &fn) {
+    if (getpid() != pid_ || workers_.empty()) return false;
+    std::unique_lock<std::mutex> busy(run_mu_, std::try_to_lock);
+    if (!busy.owns_lock()) return false;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      fn_ = &fn;
+      n_ = n;
+      nparts_ = nparts;
+      chunk_ = chunk;
+      next_.store(0);
+      done_ = 0;
+      ++gen_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> g(mu_);
+    done_cv_.wait(g, [&] { return done_ == nparts_; });
+    fn_ = nullptr;
+    return true;
+  }
+
+ private:
+  WorkerPool() : pid_(getpid()) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    for (unsigned i = 1; i < hw; ++i) workers_.emplace_back([this] { loop(); });
+  }
+  ~WorkerPool() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : workers_) t.join();
+  }
+  void work() {
+    long ndone = 0;
+    for (long i; (i = next_.fetch_add(1)) < nparts_;) {
+      const long a = i * chunk_, b = std::min(n_, a + chunk_);
+      if (a < b) (*fn_)(a, b);
+      ++ndone;
+    }
+    if (ndone) {
+      std::lock_guard<std::mutex> g(mu_);
+      done_ += ndone;
+      if (done_ == nparts_) done_cv_.notify_all();
+    }
+  }
+  void loop() {
+    unsigned long seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+      }
+      work();
+    }
+  }
+  const pid_t pid_;
+  std::vector<std::thread> workers_;
+  std::mutex run_mu_, mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(long, long)> *fn_ = nullptr;
+  long n_ = 0, nparts_ = 0, chunk_ = 0, done_ = 0;
+  std::atomic<long> next_{0};
+  unsigned long gen_ = 0;
+  bool stop_ = false;
+};
+
 static void parallel_for(long n, long grain, const std::function<void(long, long)> &fn) {
   unsigned hw = std::thread::hardware_concurrency();
   long nthreads = std::min<long>(hw ? hw : 1, (n + grain - 1) / grain);
@@ -201,14 +291,47 @@ static void parallel_for(long n, long grain, const std::function<void(long, long
     fn(0, n);
     return;
   }
+  // a few parts per thread balance uneven element costs
+  const long nparts = std::min<long>((n + grain - 1) / grain, 4 * nthreads);
+  const long chunk = (n + nparts - 1) / nparts;
+  if (WorkerPool::get().run(n, nparts, chunk, fn)) return;
   std::vector<std::thread> th;
-  long chunk = (n + nthreads - 1) / nthreads;
+  const long tchunk = (n + nthreads - 1) / nthreads;
   for (long t = 0; t < nthreads; ++t) {
-    long a = t * chunk, b = std::min(n, a + chunk);
+    long a = t * tchunk, b = std::min(n, a + tchunk);
     if (a >= b) break;
     th.emplace_back([&fn, a, b] { fn(a, b); });
   }
   for (auto &x : th) x.join();
+}
+
+// Copy `words` 64-bit limbs to pinned staging memory that the CPU will not read
+// again: streaming stores when both ends allow 16-byte vectors (no
+// read-for-ownership of the destination lines), memcpy otherwise.
+static inline void stage_limbs(uint64_t *dst, const uint64_t *src, int words) {
+#if defined(__x86_64__)
+  if (((uintptr_t)dst & 15) == 0 && (words & 1) == 0) {
+    for (int k = 0; k < words; k += 2)
+      _mm_stream_si128(reinterpret_cast<__m128i *>(dst + k),
+                       _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + k)));
+    return;
+  }
+#endif
+  memcpy(dst, src, (size_t)words * 8);
+}
+
+static inline void stage_word(int64_t *dst, int64_t v) {
+#if defined(__x86_64__)
+  _mm_stream_si64(reinterpret_cast<long long *>(dst), (long long)v);
+#else
+  *dst = v;
+#endif
+}
+
+static inline void stage_fence() {
+#if defined(__x86_64__)
+  _mm_sfence();
+#endif
 }
 
 // ---------------------------------------------------------------------------
@@ -699,26 +822,37 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
   const long emin = mpfr_get_emin(), emax = mpfr_get_emax();
   std::vector<int> nonfin(nchunks, 0);
 
+  // staging is signal-major: component u = (signal*2 + part)*Ni + q, the order
+  // the host walks the mpfr_t arrays in, so both sides stream
   auto gather = [&](unsigned long ci) {
     auto &c = p->cv[ci & 1];
     const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
     parallel_for((long)(2 * cb * Ni), 2048, [&](long x0, long x1) {
-      for (long u = x0; u < x1; ++u) {
+      constexpr long kAhead = 8;  // significands prefetched ahead of use
+      auto at = [&](long u) {
         const long bb = u / (2 * (long)Ni), part = (u / (long)Ni) & 1;
-        const unsigned long q = (unsigned long)(u % (long)Ni);
-        mpfr_srcptr x = elem(part ? ini : inr, b0 + bb, ii, q);
-        const size_t t = ((size_t)part * Ni + q) * cb + bb;
+        return elem(part ? ini : inr, b0 + bb, ii, (unsigned long)(u % (long)Ni));
+      };
+      for (long u = x0; u < std::min(x1, x0 + kAhead); ++u) __builtin_prefetch(at(u)->_mpfr_d);
+      for (long u = x0; u < x1; ++u) {
+        if (u + kAhead < x1) {
+          const mp_limb_t *d = at(u + kAhead)->_mpfr_d;
+          __builtin_prefetch(d);
+          __builtin_prefetch(d + nli - 1);
+        }
+        mpfr_srcptr x = at(u);
         if (x->_mpfr_exp <= LONG_MIN + 3) {  // MPFR's reserved exponents: zero, NaN, infinity
           if (!mpfr_zero_p(x)) nonfin[ci] = 1;
-          c.h_ei[t] = INT64_MIN;
-          c.h_si[t] = 0;
-          memset(c.h_mi + t * nli, 0, nli * 8);
+          stage_word(c.h_ei + u, INT64_MIN);
+          c.h_si[u] = 0;
+          memset(c.h_mi + u * nli, 0, nli * 8);
         } else {
-          c.h_ei[t] = x->_mpfr_exp;
-          c.h_si[t] = x->_mpfr_sign < 0;
-          memcpy(c.h_mi + t * nli, x->_mpfr_d, nli * 8);
+          stage_word(c.h_ei + u, x->_mpfr_exp);
+          c.h_si[u] = x->_mpfr_sign < 0;
+          stage_limbs(c.h_mi + u * nli, reinterpret_cast<const uint64_t *>(x->_mpfr_d), nli);
         }
       }
+      stage_fence();
     });
   };
   auto launch = [&](unsigned long ci) -> int {
@@ -728,11 +862,12 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
     CUDA_TRY(cudaMemcpyAsync(c.d_mi, c.h_mi, ci_n * nli * 8, cudaMemcpyHostToDevice, c.st));
     CUDA_TRY(cudaMemcpyAsync(c.d_ei, c.h_ei, ci_n * 8, cudaMemcpyHostToDevice, c.st));
     CUDA_TRY(cudaMemcpyAsync(c.d_si, c.h_si, ci_n, cudaMemcpyHostToDevice, c.st));
-    CUDA_TRY(mp_import_launch(c.d_mi, c.d_ei, c.d_si, nli, (int)Ni, (int)cb, p->L, p->F, c.d_es, c.d_in, c.st));
+    CUDA_TRY(mp_import_launch(c.d_mi, c.d_ei, c.d_si, nli, (int)Ni, (int)cb, p->L, p->F, c.d_es, c.d_in, c.st,
+                              true));
     uint32_t *res = nullptr;
     CUDA_TRY(mp_device_pipeline(p, mode, c.d_in, c.d_out, (int)cb, c.st, c.d_big, c.d_tmp, &res));
     CUDA_TRY(mp_export_launch(res, (int)No, (int)cb, p->L, c.d_es, p->F + fadj, prec_out, nlo, c.d_mo, c.d_eo,
-                              c.d_so, c.st));
+                              c.d_so, c.st, true));
     CUDA_TRY(cudaMemcpyAsync(c.h_mo, c.d_mo, co_n * nlo * 8, cudaMemcpyDeviceToHost, c.st));
     CUDA_TRY(cudaMemcpyAsync(c.h_eo, c.d_eo, co_n * 8, cudaMemcpyDeviceToHost, c.st));
     CUDA_TRY(cudaMemcpyAsync(c.h_so, c.d_so, co_n, cudaMemcpyDeviceToHost, c.st));
@@ -744,11 +879,20 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
     CUDA_TRY(cudaEventSynchronize(c.done));
     const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
     parallel_for((long)(2 * cb * No), 2048, [&](long x0, long x1) {
-      for (long u = x0; u < x1; ++u) {
+      constexpr long kAhead = 8;  // destination significands prefetched ahead of use
+      auto at = [&](long u) {
         const long bb = u / (2 * (long)No), part = (u / (long)No) & 1;
-        const unsigned long q = (unsigned long)(u % (long)No);
-        mpfr_ptr y = elem(part ? outi : outr, b0 + bb, oo, q);
-        const size_t t = ((size_t)part * No + q) * cb + bb;
+        return elem(part ? outi : outr, b0 + bb, oo, (unsigned long)(u % (long)No));
+      };
+      for (long u = x0; u < std::min(x1, x0 + kAhead); ++u) __builtin_prefetch(at(u)->_mpfr_d, 1);
+      for (long u = x0; u < x1; ++u) {
+        if (u + kAhead < x1) {
+          const mp_limb_t *d = at(u + kAhead)->_mpfr_d;
+          __builtin_prefetch(d, 1);
+          __builtin_prefetch(d + nlo - 1, 1);
+        }
+        mpfr_ptr y = at(u);
+        const size_t t = (size_t)u;  // signal-major staging
         const int64_t e = c.h_eo[t];
         if (e == INT64_MIN) {
           mpfr_set_zero(y, 1);

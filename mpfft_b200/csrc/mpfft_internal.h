@@ -162,10 +162,12 @@ cudaError_t mp_real_split(bool forward, int L, const uint32_t *in, uint32_t *out
 // GPU-side conversion between MPFR significands and limb planes.  Component
 // (c, p, b) is index (c*N + p)*B + b of the mant/ex/sg arrays; ex = INT64_MIN
 // marks zero.  import computes the per-signal block exponents into es[B].
+// sig_major: component (c, p, b) at index (b*2 + c)*N + p instead
 cudaError_t mp_import_launch(const uint64_t *mant, const int64_t *ex, const uint8_t *sg, int nl, int N, int B,
-                             int L, long F, int64_t *es, uint32_t *planes, cudaStream_t s);
+                             int L, long F, int64_t *es, uint32_t *planes, cudaStream_t s, bool sig_major = false);
 cudaError_t mp_export_launch(const uint32_t *planes, int N, int B, int L, const int64_t *es, long F_plus_shift,
-                             long prec, int nlo, uint64_t *out, int64_t *oex, uint8_t *osg, cudaStream_t s);
+                             long prec, int nlo, uint64_t *out, int64_t *oex, uint8_t *osg, cudaStream_t s,
+                             bool sig_major = false);
 // out[m][c][r][e] = in[m][r][c][e]: nmat matrices of R x C elements of E words
 cudaError_t transpose_launch(const uint32_t *in, uint32_t *out, long long nmat, long long R, long long C, int E,
                              cudaStream_t s);
