@@ -310,6 +310,14 @@ def main():
     imad_w = M.imad_rate(True)
     prod_peak = max(imad / 2, imad_w)  # one 32x32->64 product = lo+hi multiply-adds, or one wide
     ach_prod = sum(level_prods) / lvl_time
+    # DRAM traffic of the level launches from the committed ncu capture of this
+    # workload (one-pass metrics), per launch like `achieved`, scaled by batch
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"level_traffic_N{n}_P{p}_B2048.json")
+    if os.path.exists(tpath):
+        cap = json.load(open(tpath))
+        if len(cap["launches"]) == len(sched):
+            traffic = sum(x["dram_read"] + x["dram_write"] for x in cap["launches"]) / len(sched) * B / cap["batch"]
 
     # ---- end to end through the C ABI with host mpfr_t arrays ----
     yr, yi = mparray.MpfrArray(n * B, p), mparray.MpfrArray(n * B, p)
@@ -361,7 +369,9 @@ def main():
         "e2e": {"value": e2e, "unit": "FFT/s", "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "kernel": "mp_level_kernel", "achieved": ach_gbs, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": ach_gbs / hbm_peak, "traffic": None,
+                     "unit": "GB/s", "frac": ach_gbs / hbm_peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": sum(level_bytes) / len(sched),
+                     "traffic_source": "ncu dram__bytes_read+write, profiles/level_traffic_N1024_P1024_B2048.json",
                      "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)"},
         "roofline_compute": {"bound": "int32 multiply-add", "kernel": "mp_level_kernel",
                              "achieved": ach_prod / 1e12, "peak": prod_peak / 1e12,
