@@ -190,6 +190,18 @@ int mpfft_mp_unpack(const mpfft_mp_plan *plan, unsigned long batch, const uint32
 
 /* FP64 plans.  Host arrays: signal b at [b*n, (b+1)*n) of each array. */
 int mpfft_d_plan_create(mpfft_d_plan **plan, unsigned long n);
+/* FP64 real transforms of n real points (n a power of two >= 2; no
+ * counterpart in the reference): the n/2-point complex transform (the
+ * reference's, bit-identical) plus one split step in double.  r2c: in[b*n + j]
+ * -> X_k at outr/outi[b*(n/2+1) + k], k = 0..n/2; c2r: the inverse (sum over
+ * the Hermitian extension, imaginary parts of X_0 and X_(n/2) ignored) into
+ * out[b*n + j].  MPFFT_SCALED: times 1/n.  Rounding as a double FFT: the
+ * split step adds three roundings per bin. */
+int mpfft_d_plan_create_real(mpfft_d_plan **plan, unsigned long n);
+int mpfft_d_execute_r2c(mpfft_d_plan *plan, unsigned long batch, const double *in, double *outr, double *outi,
+                        unsigned flags);
+int mpfft_d_execute_c2r(mpfft_d_plan *plan, unsigned long batch, const double *inr, const double *ini, double *out,
+                        unsigned flags);
 /* FP64 multi-dimensional plan (rank 1..3, row-major, at most 2^28 points): the
  * reference's double transform along each axis in turn, last axis first,
  * each bit-identical to d_sr24_cp_fft; layout [c][b][p] with p the row-major

@@ -71,6 +71,9 @@ def _load() -> C.CDLL:
         "mpfft_mp_plan_create_real": (C.c_int, [C.POINTER(vp), ul, sl, C.c_uint]),
         "mpfft_mp_plan_create_nd": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(ul), sl, C.c_uint]),
         "mpfft_d_plan_create_nd": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(ul)]),
+        "mpfft_d_plan_create_real": (C.c_int, [C.POINTER(vp), ul]),
+        "mpfft_d_execute_r2c": (C.c_int, [vp, ul, dp, dp, dp, C.c_uint]),
+        "mpfft_d_execute_c2r": (C.c_int, [vp, ul, dp, dp, dp, C.c_uint]),
         "mpfft_mp_execute_r2c": (C.c_int, [vp, ul, vp, vp, vp, C.c_uint]),
         "mpfft_mp_execute_c2r": (C.c_int, [vp, ul, vp, vp, vp, C.c_uint]),
         "mpfft_mp_pack": (C.c_int, [vp, ul, vp, vp, u32p, vp]),
@@ -310,6 +313,22 @@ class DPlan:
 
     def execute_device(self, batch, d_in: int, d_out: int, scaled=False, stream: int = 0) -> None:
         _check(lib.mpfft_d_execute_device(self.h, batch, d_in, d_out, SCALED if scaled else 0, stream or None))
+
+
+class DRealPlan(DPlan):
+    """FP64 real transform of n real points (n/2+1-point half spectrum)."""
+
+    def __init__(self, n: int):
+        h = C.c_void_p()
+        _check(lib.mpfft_d_plan_create_real(C.byref(h), n))
+        self.h = h
+        self.n = n
+
+    def r2c(self, batch, x, outr, outi, scaled=False) -> None:
+        _check(lib.mpfft_d_execute_r2c(self.h, batch, _dp(x), _dp(outr), _dp(outi), SCALED if scaled else 0))
+
+    def c2r(self, batch, inr, ini, x, scaled=False) -> None:
+        _check(lib.mpfft_d_execute_c2r(self.h, batch, _dp(inr), _dp(ini), _dp(x), SCALED if scaled else 0))
 
 
 class DPlanND(DPlan):

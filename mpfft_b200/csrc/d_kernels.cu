@@ -347,6 +347,80 @@ __global__ void __launch_bounds__(256) d_level_kernel(double *__restrict__ y, in
   d_butterfly(y + (size_t)b * N, y + ((size_t)B + b) * N, 1, node_off[node], k, q, wr[kn], wi[kn], scale);
 }
 
+// Split step of the FP64 real transforms (n = 2M real points; layouts [c][b][k]).
+// Forward: Z = FFT_M(x_2m + i x_2m+1) (M points) -> X_0..X_M (M+1 points):
+//   S = Z_k + conj Z_(M-k), D = Z_k - conj Z_(M-k), T = w^k D (w = exp(-2 pi i/n)),
+//   X_k = (S_r + T_i, S_i - T_r) / 2,  X_(M-k) = (S_r - T_i, -(S_i + T_r)) / 2.
+// Inverse: X (M+1 points) -> W = the planes-exchanged 2Z, with
+//   S' = X_k + conj X_(M-k), D' = X_k - conj X_(M-k), T' = w^-k D',
+//   2Z_k = (S'_r - T'_i, S'_i + T'_r), 2Z_(M-k) = (S'_r + T'_i, T'_r - S'_i),
+// so that the forward transform of W is n * (x_2m+1 + i x_2m) (the swap
+// identity); the imaginary parts of X_0 and X_M are ignored.  wc, ws: cos and
+// sin of 2 pi k/n for k < M/2; scale multiplies the forward outputs.
+__global__ void __launch_bounds__(256) d_r2c_post(const double *__restrict__ z, double *__restrict__ x, int M, int B,
+                                                   const double *__restrict__ wc, const double *__restrict__ ws,
+                                                   double scale) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)(M / 2 + 1) * B) return;
+  const int k = (int)(t % (M / 2 + 1));
+  const int b = (int)(t / (M / 2 + 1));
+  const double *zr = z + (size_t)b * M, *zi = z + ((size_t)B + b) * M;
+  double *xr = x + (size_t)b * (M + 1), *xi = x + ((size_t)B + b) * (M + 1);
+  const double h = 0.5 * scale;
+  if (k == 0) {
+    xr[0] = (zr[0] + zi[0]) * scale;
+    xi[0] = 0.0;
+    xr[M] = (zr[0] - zi[0]) * scale;
+    xi[M] = 0.0;
+    return;
+  }
+  const double ar = zr[k], ai = zi[k], br = zr[M - k], bi = zi[M - k];
+  const double sr = ar + br, si = ai - bi, dr = ar - br, di = ai + bi;
+  const double c = 2 * k == M ? 0.0 : wc[k], s = 2 * k == M ? 1.0 : ws[k];
+  const double tr = c * dr + s * di, ti = c * di - s * dr;
+  xr[k] = (sr + ti) * h;
+  xi[k] = (si - tr) * h;
+  if (2 * k != M) {
+    xr[M - k] = (sr - ti) * h;
+    xi[M - k] = -(si + tr) * h;
+  }
+}
+
+__global__ void __launch_bounds__(256) d_c2r_pre(const double *__restrict__ x, double *__restrict__ w, int M, int B,
+                                                  const double *__restrict__ wc, const double *__restrict__ ws) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)(M / 2 + 1) * B) return;
+  const int k = (int)(t % (M / 2 + 1));
+  const int b = (int)(t / (M / 2 + 1));
+  const double *xr = x + (size_t)b * (M + 1), *xi = x + ((size_t)B + b) * (M + 1);
+  // W = (2Z_i, 2Z_r): real plane holds the imaginary parts
+  double *wr = w + (size_t)b * M, *wi = w + ((size_t)B + b) * M;
+  if (k == 0) {
+    wi[0] = xr[0] + xr[M];
+    wr[0] = xr[0] - xr[M];
+    return;
+  }
+  const double ar = xr[k], ai = xi[k], br = xr[M - k], bi = xi[M - k];
+  const double sr = ar + br, si = ai - bi, dr = ar - br, di = ai + bi;
+  const double c = 2 * k == M ? 0.0 : wc[k], s = 2 * k == M ? 1.0 : ws[k];
+  const double tr = c * dr - s * di, ti = c * di + s * dr;
+  wi[k] = sr - ti;
+  wr[k] = si + tr;
+  if (2 * k != M) {
+    wi[M - k] = sr + ti;
+    wr[M - k] = tr - si;
+  }
+}
+
+cudaError_t d_real_split(bool forward, const double *in, double *out, int M, int B, const double *wc,
+                         const double *ws, double scale, cudaStream_t s) {
+  const long long total = (long long)(M / 2 + 1) * B;
+  const int blocks = (int)((total + 255) / 256);
+  if (forward) d_r2c_post<<<blocks, 256, 0, s>>>(in, out, M, B, wc, ws, scale);
+  else d_c2r_pre<<<blocks, 256, 0, s>>>(in, out, M, B, wc, ws);
+  return cudaGetLastError();
+}
+
 // instances of the shared-memory kernel per CTA and its dynamic shared memory
 static int d_sub_instances(const DDeviceTables &T) {
   if (T.nroots != 1) return 1;

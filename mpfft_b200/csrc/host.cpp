@@ -479,8 +479,11 @@ struct mpfft_d_plan {
   int rank = 1;
   unsigned long dims[3] = {0, 0, 0};
   std::unique_ptr<mpfft_d_plan> axis[3];
-  double *d_tmp = nullptr;  // rank > 1: transposition buffer, grown on demand
+  double *d_tmp = nullptr;  // rank > 1: transposition buffer; real plans: split-step output
   size_t tmp_cap = 0;
+  bool real = false;        // real transform of n_real = 2N points: N-point complex transform + split step
+  unsigned long n_real = 0;
+  double *d_wc = nullptr, *d_ws = nullptr;  // real plans: cos, sin of 2 pi k / n_real, k < N/2
   DeviceTree upper;                   // levels above the shared-memory sub-transforms
   std::vector<void *> dev_allocs;     // roots, perms, sub-schedule tables
   double *d_wr = nullptr, *d_wi = nullptr;
@@ -498,6 +501,8 @@ struct mpfft_d_plan {
     if (h_in) cudaFreeHost(h_in);
     if (h_out) cudaFreeHost(h_out);
     if (d_tmp) cudaFree(d_tmp);
+    if (d_wc) cudaFree(d_wc);
+    if (d_ws) cudaFree(d_ws);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -1151,7 +1156,7 @@ static mpfft_d_plan *d_cached(unsigned long n) {
 }
 
 static int d_reserve(mpfft_d_plan *p, unsigned long batch) {
-  const size_t words = (size_t)2 * p->N * batch;
+  const size_t words = (size_t)2 * (p->real ? p->N + 1 : p->N) * batch;
   if (words <= p->cap) return MPFFT_OK;
   if (p->d_in) cudaFree(p->d_in);
   if (p->d_out) cudaFree(p->d_out);
@@ -1222,8 +1227,8 @@ static cudaError_t d_transform(mpfft_d_plan *p, const double *in, double *out, i
 
 static int d_tmp_reserve(mpfft_d_plan *p, unsigned long batch, double **out) {
   *out = nullptr;
-  if (p->rank == 1) return MPFFT_OK;
-  const size_t words = (size_t)2 * p->N * batch;
+  if (p->rank == 1 && !p->real) return MPFFT_OK;
+  const size_t words = (size_t)2 * (p->real ? p->N + 1 : p->N) * batch;
   if (words > p->tmp_cap) {
     if (p->d_tmp) cudaFree(p->d_tmp);
     p->d_tmp = nullptr;
@@ -1265,6 +1270,68 @@ static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *in
   CUDA_TRY(cudaStreamSynchronize(p->stream));
   memcpy(outr, p->h_out, cim * sizeof(double));
   memcpy(outi, p->h_out + cim, cim * sizeof(double));
+  return set_err(MPFFT_OK, "");
+}
+
+// real transform of n >= 2 points: the n/2-point complex plan plus split twiddles
+static int d_plan_init_real(mpfft_d_plan *p, unsigned long n) {
+  if (!is_pow2(n) || n < 2) return set_err(MPFFT_EINVAL, "a real transform needs n >= 2, a power of two (n=%lu)", n);
+  if (n > (1UL << 28)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
+  if (int e = d_plan_init(p, n / 2)) return e;
+  p->real = true;
+  p->n_real = n;
+  const unsigned long q = std::max<unsigned long>(1, n / 4);
+  std::vector<double> wc(q), ws(q);
+  for (unsigned long k = 0; k < q; ++k) {
+    wc[k] = cos(2. * M_PI * k / n);
+    ws[k] = sin(2. * M_PI * k / n);
+  }
+  CUDA_TRY(cudaMalloc(&p->d_wc, q * sizeof(double)));
+  CUDA_TRY(cudaMalloc(&p->d_ws, q * sizeof(double)));
+  CUDA_TRY(cudaMemcpy(p->d_wc, wc.data(), q * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(p->d_ws, ws.data(), q * sizeof(double), cudaMemcpyHostToDevice));
+  return MPFFT_OK;
+}
+
+// forward: in = batch x n reals -> outr/outi = batch x (n/2+1); else the inverse
+static int d_execute_real(mpfft_d_plan *p, bool forward, unsigned long batch, const double *xin, const double *inr,
+                          const double *ini, double *xout, double *outr, double *outi, unsigned flags) {
+  std::lock_guard<std::mutex> g(p->mu);
+  const unsigned long M = p->N, n = p->n_real, H = M + 1;
+  if ((unsigned long long)batch * H > (unsigned long long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  if (int e = d_reserve(p, batch)) return e;
+  double *tmp = nullptr;
+  if (int e = d_tmp_reserve(p, batch, &tmp)) return e;
+  const double scale = (flags & MPFFT_SCALED) ? 1.0 / (double)n : 1.0;
+  if (forward) {
+    // even samples -> real plane, odd samples -> imaginary plane ([c][b][m])
+    for (unsigned long b = 0; b < batch; ++b)
+      for (unsigned long m = 0; m < M; ++m) {
+        p->h_in[b * M + m] = xin[b * n + 2 * m];
+        p->h_in[(batch + b) * M + m] = xin[b * n + 2 * m + 1];
+      }
+    CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, 2 * M * batch * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    CUDA_TRY(d_run_transform(p->tabs, p->d_in, p->d_out, (int)batch, 1.0, p->stream));
+    CUDA_TRY(d_real_split(true, p->d_out, tmp, (int)M, (int)batch, p->d_wc, p->d_ws, scale, p->stream));
+    CUDA_TRY(cudaMemcpyAsync(p->h_out, tmp, 2 * H * batch * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    CUDA_TRY(cudaStreamSynchronize(p->stream));
+    memcpy(outr, p->h_out, H * batch * sizeof(double));
+    memcpy(outi, p->h_out + H * batch, H * batch * sizeof(double));
+  } else {
+    memcpy(p->h_in, inr, H * batch * sizeof(double));
+    memcpy(p->h_in + H * batch, ini, H * batch * sizeof(double));
+    CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, 2 * H * batch * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    CUDA_TRY(d_real_split(false, p->d_in, tmp, (int)M, (int)batch, p->d_wc, p->d_ws, 1.0, p->stream));
+    CUDA_TRY(d_run_transform(p->tabs, tmp, p->d_out, (int)batch, scale, p->stream));
+    CUDA_TRY(cudaMemcpyAsync(p->h_out, p->d_out, 2 * M * batch * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    CUDA_TRY(cudaStreamSynchronize(p->stream));
+    // the transform of the exchanged planes: imaginary plane = even samples
+    for (unsigned long b = 0; b < batch; ++b)
+      for (unsigned long m = 0; m < M; ++m) {
+        xout[b * n + 2 * m] = p->h_out[(batch + b) * M + m];
+        xout[b * n + 2 * m + 1] = p->h_out[b * M + m];
+      }
+  }
   return set_err(MPFFT_OK, "");
 }
 
@@ -1505,6 +1572,32 @@ MPFFT_API int mpfft_d_plan_create(mpfft_d_plan **plan, unsigned long n) {
   return set_err(MPFFT_OK, "");
 }
 
+MPFFT_API int mpfft_d_plan_create_real(mpfft_d_plan **plan, unsigned long n) {
+  if (!plan) return set_err(MPFFT_EINVAL, "NULL plan pointer");
+  *plan = nullptr;
+  std::unique_ptr<mpfft_d_plan> p(new (std::nothrow) mpfft_d_plan);
+  if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
+  if (int e = d_plan_init_real(p.get(), n)) return e;
+  *plan = p.release();
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_d_execute_r2c(mpfft_d_plan *plan, unsigned long batch, const double *in, double *outr,
+                                  double *outi, unsigned flags) {
+  if (!plan || !in || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (!plan->real) return set_err(MPFFT_EINVAL, "not a real plan (mpfft_d_plan_create_real)");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  return d_execute_real(plan, true, batch, in, nullptr, nullptr, nullptr, outr, outi, flags);
+}
+
+MPFFT_API int mpfft_d_execute_c2r(mpfft_d_plan *plan, unsigned long batch, const double *inr, const double *ini,
+                                  double *out, unsigned flags) {
+  if (!plan || !inr || !ini || !out) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (!plan->real) return set_err(MPFFT_EINVAL, "not a real plan (mpfft_d_plan_create_real)");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  return d_execute_real(plan, false, batch, nullptr, inr, ini, out, nullptr, nullptr, flags);
+}
+
 MPFFT_API int mpfft_d_plan_create_nd(mpfft_d_plan **plan, int rank, const unsigned long *dims) {
   if (!plan) return set_err(MPFFT_EINVAL, "NULL plan pointer");
   *plan = nullptr;
@@ -1523,6 +1616,7 @@ MPFFT_API int mpfft_d_plan_destroy(mpfft_d_plan *plan) {
 MPFFT_API int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const double *inr, const double *ini,
                               double *outr, double *outi, unsigned flags) {
   if (!plan || !inr || !ini || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (plan->real) return set_err(MPFFT_EINVAL, "real plan: use mpfft_d_execute_r2c / mpfft_d_execute_c2r");
   if (batch == 0) return set_err(MPFFT_OK, "");
   if (flags & MPFFT_INVERSE) {  // ifft(X) = swap(FFT(swap(X))) (times 1/n if scaled)
     std::swap(inr, ini);
@@ -1535,6 +1629,7 @@ MPFFT_API int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const dou
 MPFFT_API int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, const double *d_in, double *d_out,
                                      unsigned flags, void *stream) {
   if (!plan || !d_in || !d_out) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (plan->real) return set_err(MPFFT_EINVAL, "real plans have no device-layout entry point");
   if (batch == 0) return set_err(MPFFT_OK, "");
   const size_t bytes = (size_t)2 * plan->N * batch * 8;
   const char *a = (const char *)d_in, *b = (const char *)d_out;

@@ -174,6 +174,9 @@ cudaError_t transpose_launch(const uint32_t *in, uint32_t *out, long long nmat, 
 // FP64 layout: word (c, b, p) at base[(c*B + b)*N + p]  (signal-contiguous)
 cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
                             cudaStream_t s);
+// split step of the FP64 real transforms (n = 2M real points), d_kernels.cu
+cudaError_t d_real_split(bool forward, const double *in, double *out, int M, int B, const double *wc,
+                         const double *ws, double scale, cudaStream_t s);
 
 // Import -> transform -> export of device-resident MPFR fields with all
 // working storage in a file-scope device array (static_scratch.cu).  Returns an

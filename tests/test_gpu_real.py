@@ -7,6 +7,7 @@ Acceptance as for the complex path: normwise relative error against a direct
 MPFR DFT at 2P bits <= 8*log2(N)*2^-P, and no worse than the reference's
 complex transform at the same P (first N/2+1 bins).
 """
+import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -153,3 +154,50 @@ def test_real_errors(M, orc):
     cplx = M.MpPlan(n, p)
     assert M.lib.mpfft_mp_execute_r2c(cplx.h, 1, x.ptr, yr.ptr, yi.ptr, 0) == M.EINVAL
     assert M.lib.mpfft_mp_execute(plan.h, 1, x.ptr, x.ptr, yr.ptr, yi.ptr, 0) == M.EINVAL
+
+
+# ---------------------------------------------------------------------------
+# FP64 real transforms
+# ---------------------------------------------------------------------------
+
+def _rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+@pytest.mark.parametrize("n", [2, 4, 8, 64, 1024, 4096, 1 << 16])
+def test_d_r2c_c2r(M, orc, n):
+    """Against numpy's pocketfft and against the reference's complex double
+    transform (our bit-exact restatement) of the zero-imaginary signal, within
+    a few units of double rounding; c2r(r2c(x)) = x."""
+    O = orc
+    batch, m = 3, n // 2
+    rng = np.random.default_rng(n)
+    x = rng.uniform(-1, 1, size=(batch, n))
+    plan = M.DRealPlan(n)
+    yr, yi = np.zeros((batch, m + 1)), np.zeros((batch, m + 1))
+    plan.r2c(batch, x, yr, yi)
+    tol = 8 * max(1, np.log2(n)) * 2.0 ** -53
+    ref = np.fft.rfft(x, axis=1)
+    assert _rel(yr + 1j * yi, ref) <= tol
+    assert np.all(yi[:, 0] == 0) and np.all(yi[:, m] == 0)
+    f = O.DFFT(n)
+    for b in range(batch):
+        cr, ci = f(x[b].copy(), np.zeros(n))
+        assert _rel(yr[b] + 1j * yi[b], cr[: m + 1] + 1j * ci[: m + 1]) <= tol
+    # scaled forward, unscaled inverse: the round trip
+    sr, si = np.zeros_like(yr), np.zeros_like(yi)
+    plan.r2c(batch, x, sr, si, scaled=True)
+    back = np.zeros_like(x)
+    plan.c2r(batch, sr, si, back)
+    assert _rel(back, x) <= tol
+    # c2r of a random half spectrum vs numpy's irfft (times n), imaginary parts of X_0, X_m ignored
+    hr, hi = rng.uniform(-1, 1, size=(batch, m + 1)), rng.uniform(-1, 1, size=(batch, m + 1))
+    out = np.zeros((batch, n))
+    plan.c2r(batch, hr, hi, out)
+    h = hr + 1j * hi
+    h[:, 0] = h[:, 0].real
+    h[:, m] = h[:, m].real
+    assert _rel(out, np.fft.irfft(h, n=n, axis=1) * n) <= tol
+    scaled = np.zeros((batch, n))
+    plan.c2r(batch, hr, hi, scaled, scaled=True)
+    assert np.array_equal(scaled, out / n)
