@@ -56,6 +56,7 @@ extern "C" {
 #define MPFFT_PLAN_HOST_CONVERSION 4u /* plan creation: convert mpfr_t <-> limbs on the host, not the GPU */
 #define MPFFT_PLAN_NO_TENSOR 16u /* plan creation: keep large-precision twiddle products on the integer
                                      pipes (by default 35..260 limbs use int8 tensor-core GEMMs) */
+#define MPFFT_PLAN_TENSOR 32u    /* plan creation: tensor-core twiddle products from 8 limbs up */
 
 /* ------------------------------------------------------------------------ */
 /* 1. drop-in replacements for mpFFT.h                                      */

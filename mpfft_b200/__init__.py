@@ -29,6 +29,7 @@ PLAN_HOST_ONLY = 2
 PLAN_HOST_CONVERSION = 4
 INVERSE = 8
 PLAN_NO_TENSOR = 16
+PLAN_TENSOR = 32
 
 
 class MpfftError(RuntimeError):
@@ -173,10 +174,12 @@ class MpPlan:
     """Multiprecision plan for n points at `prec` bits (device limb format)."""
 
     def __init__(self, n: int, prec: int, host_only: bool = False, host_conversion: bool = False,
-                 tensor: bool = True):
+                 tensor=True):
+        """tensor: True (default choice), False (integer pipes only) or
+        "force" (tensor-core products from 8 limbs up)."""
         h = C.c_void_p()
         flags = ((PLAN_HOST_ONLY if host_only else 0) | (PLAN_HOST_CONVERSION if host_conversion else 0)
-                 | (0 if tensor else PLAN_NO_TENSOR))
+                 | (PLAN_TENSOR if tensor == "force" else 0 if tensor else PLAN_NO_TENSOR))
         _check(lib.mpfft_mp_plan_create_flags(C.byref(h), n, prec, flags))
         self.h = h
         self.n, self.prec = n, prec

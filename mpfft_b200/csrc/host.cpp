@@ -700,7 +700,8 @@ static void mp_fill_nan(mpfr_t *a, unsigned long n) {
 
 // streaming/tensor-kernel scratch words of one transform of B signals (0 when unused)
 static size_t mp_plan_big_words(const mpfft_mp_plan *p, unsigned long B) {
-  if (p->L <= kMaxLimbs) return 0;
+  const MpDeviceTables &T0 = p->rank > 1 ? p->axis[0]->tabs : p->tabs;
+  if (p->L <= kMaxLimbs && !mp_tc_used(T0, p->L)) return 0;
   if (p->rank == 1) return mp_big_scratch_words(p->tabs, p->L, (int)B);
   size_t w = 0;
   for (int s = 0; s < p->rank; ++s)
@@ -755,7 +756,7 @@ static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int n
     dm((void **)&c.d_so, comp);
     hm((void **)&c.h_so, comp);
     dm((void **)&c.d_es, chunk * 8);
-    if (p->L > kMaxLimbs) dm((void **)&c.d_big, mp_plan_big_words(p, chunk) * 4);
+    if (const size_t bw = mp_plan_big_words(p, chunk)) dm((void **)&c.d_big, bw * 4);
     if (p->rank > 1) dm((void **)&c.d_tmp, words * 4);
   }
   if (!ok) {
@@ -940,8 +941,8 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
 // streaming-kernel scratch for a batch (large limb counts only); null otherwise
 static int mp_big_reserve(mpfft_mp_plan *p, unsigned long batch, uint32_t **out) {
   *out = nullptr;
-  if (p->L <= kMaxLimbs) return MPFFT_OK;
   const size_t words = mp_plan_big_words(p, batch);
+  if (words == 0) return MPFFT_OK;
   if (words > p->big_words) {
     if (p->d_big) cudaFree(p->d_big);
     p->d_big = nullptr;
@@ -1432,6 +1433,7 @@ MPFFT_API int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, 
   if (int e = mp_plan_init(p.get(), n, prec, (flags & MPFFT_PLAN_HOST_ONLY) != 0)) return e;
   p->force_host_conversion = (flags & MPFFT_PLAN_HOST_CONVERSION) != 0;
   if (flags & MPFFT_PLAN_NO_TENSOR) p->tabs.tc = 0;
+  else if (flags & MPFFT_PLAN_TENSOR) p->tabs.tc = 2;
   *plan = p.release();
   return set_err(MPFFT_OK, "");
 }
@@ -1444,10 +1446,11 @@ MPFFT_API int mpfft_mp_plan_create_nd(mpfft_mp_plan **plan, int rank, const unsi
   if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
   if (int e = mp_plan_init_nd(p.get(), rank, dims, prec, (flags & MPFFT_PLAN_HOST_ONLY) != 0)) return e;
   p->force_host_conversion = (flags & MPFFT_PLAN_HOST_CONVERSION) != 0;
-  if (flags & MPFFT_PLAN_NO_TENSOR) {
-    p->tabs.tc = 0;
+  if (flags & (MPFFT_PLAN_NO_TENSOR | MPFFT_PLAN_TENSOR)) {
+    const int tc = (flags & MPFFT_PLAN_NO_TENSOR) ? 0 : 2;
+    p->tabs.tc = tc;
     for (auto &a : p->axis)
-      if (a) a->tabs.tc = 0;
+      if (a) a->tabs.tc = tc;
   }
   *plan = p.release();
   return set_err(MPFFT_OK, "");
@@ -1713,8 +1716,9 @@ MPFFT_API int mpfft_mp_execute_significands_static(const mpfft_mp_plan *plan, un
   if (nl_in < 1 || prec_out < 2) return set_err(MPFFT_EINVAL, "nl_in must be >= 1 and prec_out >= 2");
   if (batch == 0) return set_err(MPFFT_OK, "");
   if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");
-  if (plan->L > kMaxLimbs)
-    return set_err(MPFFT_EUNSUPPORTED, "the static-scratch entry point supports up to %d limbs (plan has %d)",
+  if (plan->L > kMaxLimbs || mp_tc_used(plan->tabs, plan->L))
+    return set_err(MPFFT_EUNSUPPORTED,
+                   "the static-scratch entry point supports up to %d limbs on the integer kernels (plan has %d)",
                    kMaxLimbs, plan->L);
   MpPlanView v;
   v.N = plan->N;

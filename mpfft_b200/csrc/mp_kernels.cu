@@ -278,7 +278,7 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
 
 cudaError_t mp_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
                              cudaStream_t s, float *launch_ms, uint32_t *big_scratch) {
-  if (L > kMaxLimbs) {
+  if (L > kMaxLimbs || mp_tc_used(T, L)) {
     if (!big_scratch || L > kMaxLimbsBig) return cudaErrorInvalidValue;
     return mp_big_run_transform(L, T, in, out, B, big_scratch, s, launch_ms);
   }

@@ -36,9 +36,9 @@
 // Pipeline inside a CTA (128 threads, one per signal): operand bytes are
 // written to shared memory by all threads; thread 0 issues the MMAs of one
 // output tile into one of two 128-column tensor-memory buffers and commits
-// them to that buffer's mbarrier; while the epilogue drains tile t, the MMAs
-// of tile t+1 run.  Every wait is bounded (about two seconds of %globaltimer);
-// on expiry the kernel records an error code instead of hanging.
+// them to that buffer's mbarrier; while the threads drain tile t (32 columns
+// at a time), the MMAs of tile t+1 run.  Every wait is bounded (about two seconds of %globaltimer); on
+// expiry the kernel records an error code instead of hanging.
 #include <cstdint>
 
 #include "mp_stream.cuh"
@@ -47,8 +47,14 @@
 namespace mpfft {
 
 constexpr int kTcRows = 128;                    // signals per CTA (MMA M)
-constexpr uint32_t kTcMinSmem = 80u * 1024u;    // at most two CTAs per SM: 2 x 256 TMEM columns
-constexpr uint32_t kTcTmemCols = 256;           // two 128-column accumulator buffers
+
+// Tensor memory per CTA: two 128-column accumulators (the MMAs of tile t+1
+// overlap the drain of tile t).  At least 80 KB of shared memory per CTA keeps
+// a third CTA off the SM, so 2 x 256 of the 512 columns suffice and an
+// allocation never waits.  (Measured: four CTAs per SM with one accumulator
+// each and at most 128 registers per thread was slower from 65 limbs up.)
+constexpr uint32_t kTcMinSmem = 80u * 1024u;
+constexpr uint32_t kTcTmemCols = 256;
 // instruction descriptor: D = s32, A = B = u8, both K-major, N = 128, M = 128
 constexpr uint32_t kTcIdesc = (2u << 4) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 
@@ -214,7 +220,7 @@ __device__ void tc_build_twiddle(TcCtx &c, int which, const uint32_t *w, size_t 
 // |pa +/- pb| (pb may be null) of this thread's signal into operand row m of
 // the CTA (4L bytes, zero padded to Kpad); returns its sign (1 = negative).
 // Rows of signals beyond the batch read signal 0 (the caller clamps the
-// pointers); their products are never stored.  Loads are unconditional, 16
+// pointers); their products are never stored.  Loads are unconditional, kB
 // limbs of each input in flight.
 __device__ uint32_t tc_prep(TcCtx &c, const uint32_t *pa, const uint32_t *pb, size_t plane, bool sub) {
   const TcGeom &G = c.G;
@@ -411,7 +417,6 @@ __device__ void tc_product(TcCtx &c, int which, TcEmit &em) {
     tc_fence_after();
     tc_issue(c, which, 0, c.counter & 1);
   }
-  __syncwarp();
   for (int t = 0; t < G.nt; ++t) {
     const int buf = (c.counter + t) & 1;
     if (threadIdx.x == 0 && t + 1 < G.nt) tc_issue(c, which, t + 1, buf ^ 1);
@@ -419,23 +424,27 @@ __device__ void tc_product(TcCtx &c, int which, TcEmit &em) {
     if (!c.bad && !mbar_wait(c.bar + 8u * buf, (c.ph >> buf) & 1u)) c.bad = true;
     c.ph ^= 1u << buf;
     tc_fence_after();
-    uint32_t v[128];
-    MPFFT_TMEM_LD32(lane_addr + buf * 128u + 0u, v);
-    MPFFT_TMEM_LD32(lane_addr + buf * 128u + 32u, v + 32);
-    MPFFT_TMEM_LD32(lane_addr + buf * 128u + 64u, v + 64);
-    MPFFT_TMEM_LD32(lane_addr + buf * 128u + 96u, v + 96);
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    // Tile column n = 8g + r holds output byte column J + g + 16(7 - r), so
+    // 32-column chunk ch holds the 4 bytes e of the 8 limb columns
+    // lc = ch + 4(7 - r) at columns 8e + r: fold each chunk into limb-column
+    // sums S[lc] = sum_e D[4 lc + e] 2^(8e) (< 2^52) as it arrives.
+    uint64_t S[32];
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+      uint32_t v[32];
+      MPFFT_TMEM_LD32(lane_addr + 128u * buf + 32u * ch, v);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        S[ch + 4 * (7 - r)] = (uint64_t)v[r] + (uint64_t)v[8 + r] * 0x100u + (uint64_t)v[16 + r] * 0x10000u +
+                              (uint64_t)v[24 + r] * 0x1000000u;
+    }
     const int mbase = (G.J0 >> 2) + 32 * t;  // limb column of this tile's first byte column
 #pragma unroll
     for (int lc = 0; lc < 32; ++lc) {
       const int m = mbase + lc;
       if (m >= 2 * L) break;  // above the product's top limb
-      // output column J + jj sits in row n = 8 (jj mod 16) + 7 - jj/16 of the tile
-      uint64_t sum = carry;
-      sum += (uint64_t)v[8 * ((4 * lc) & 15) + 7 - ((4 * lc) >> 4)];
-      sum += (uint64_t)v[8 * ((4 * lc + 1) & 15) + 7 - ((4 * lc + 1) >> 4)] * 0x100u;
-      sum += (uint64_t)v[8 * ((4 * lc + 2) & 15) + 7 - ((4 * lc + 2) >> 4)] * 0x10000u;
-      sum += (uint64_t)v[8 * ((4 * lc + 3) & 15) + 7 - ((4 * lc + 3) >> 4)] * 0x1000000u;
+      uint64_t sum = S[lc] + carry;
       if (m == L - 1) sum += 1ull << 30;  // + 2^(32L-2): round to nearest
       const uint32_t limb = (uint32_t)sum;
       carry = sum >> 32;

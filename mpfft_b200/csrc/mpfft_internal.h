@@ -40,7 +40,8 @@ struct MpDeviceTables : TreeTables {
   const uint32_t *tw = nullptr;   // [3][L][tws*N/4]: cos, cos+sin, |cos-sin| magnitudes
   const uint8_t *dneg = nullptr;  // [tws*N/4]: sign of cos-sin
   int tws = 1;  // the table is built for tws*N points (2 for a real transform of 2N points)
-  int tc = 1;   // large limb counts: twiddle products on the tensor cores (mp_tc_kernels.cu)
+  int tc = 1;   // twiddle products on the tensor cores (mp_tc_kernels.cu): 0 never, 1 from
+                // kTcMinLimbs limbs, 2 from kTcForceMinLimbs limbs
 };
 
 // Schedule of one shared-memory sub-transform of size `size` (FP64 tier):
@@ -101,6 +102,7 @@ constexpr int kMinLimbs = 2;
 // over the whole range
 constexpr int kTcMinLimbs = 35;
 constexpr int kTcMaxLimbs = 260;
+constexpr int kTcForceMinLimbs = 8;
 
 // launch_ms (optional, host array of >= 1 + nlevels floats): when non-null,
 // each launch is bracketed by events on `s` and its duration written there
@@ -152,7 +154,9 @@ cudaError_t mp_tc_mul(int L, int B, const uint32_t *x, const uint32_t *w, uint32
 // reads and clears the device-side error flag of the tensor-core kernels
 cudaError_t mp_tc_take_error(int *code);
 size_t mp_tc_smem_bytes(int L);
-inline bool mp_tc_used(const MpDeviceTables &T, int L) { return T.tc && L >= kTcMinLimbs && L <= kTcMaxLimbs; }
+inline bool mp_tc_used(const MpDeviceTables &T, int L) {
+  return T.tc && L >= (T.tc == 2 ? kTcForceMinLimbs : kTcMinLimbs) && L <= kTcMaxLimbs;
+}
 // Split step of a real transform of 2M points (L <= kMaxLimbs; tw/dneg: the
 // table of a 2M-point plan).  forward: Z (M points) -> 2X (M+1 points);
 // otherwise half spectrum X (M+1 points) -> 2Z with its planes exchanged.

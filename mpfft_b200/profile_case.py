@@ -68,11 +68,12 @@ def main():
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--no-tensor", action="store_true", help="large precision: integer-pipe products")
+    ap.add_argument("--force-tensor", action="store_true", help="tensor-core products from 8 limbs up")
     a = ap.parse_args()
     if a.tier == "fp64":
         run_fp64(a)
         return
-    plan = M.MpPlan(a.n, a.prec, tensor=not a.no_tensor)
+    plan = M.MpPlan(a.n, a.prec, tensor="force" if a.force_tensor else not a.no_tensor)
     host = synthetic_planes(a.n, plan.limbs, plan.frac_bits, a.batch)
     d_in = torch.from_numpy(host.view(np.int32)).cuda()
     d_out = torch.empty_like(d_in)
