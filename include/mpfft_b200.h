@@ -51,7 +51,8 @@ extern "C" {
 
 /* flags */
 #define MPFFT_SCALED 1u         /* execute: multiply the result by 1/n (exact) */
-#define MPFFT_INVERSE 8u        /* execute (host arrays): backward transform, exp(+2 pi i jk/n) */
+#define MPFFT_INVERSE 8u        /* execute (host arrays, FP64 device planes): backward transform,
+                                   exp(+2 pi i jk/n); unscaled it is the adjoint (conjugate transpose) */
 #define MPFFT_PLAN_HOST_ONLY 2u /* plan creation: conversion (pack/unpack) only, no device state */
 #define MPFFT_PLAN_HOST_CONVERSION 4u /* plan creation: convert mpfr_t <-> limbs on the host, not the GPU */
 #define MPFFT_PLAN_NO_TENSOR 16u /* plan creation: keep large-precision twiddle products on the integer

@@ -314,8 +314,9 @@ class DPlan:
         flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
         _check(lib.mpfft_d_execute(self.h, batch, _dp(inr), _dp(ini), _dp(outr), _dp(outi), flags))
 
-    def execute_device(self, batch, d_in: int, d_out: int, scaled=False, stream: int = 0) -> None:
-        _check(lib.mpfft_d_execute_device(self.h, batch, d_in, d_out, SCALED if scaled else 0, stream or None))
+    def execute_device(self, batch, d_in: int, d_out: int, scaled=False, stream: int = 0, inverse=False) -> None:
+        flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
+        _check(lib.mpfft_d_execute_device(self.h, batch, d_in, d_out, flags, stream or None))
 
 
 class DRealPlan(DPlan):

@@ -180,8 +180,9 @@ __device__ __forceinline__ void d_leaf_small(double *yr, double *yi, int o, int 
 }
 
 // 4m2a butterfly k of a node of size n at y[off..) (reference :392-427)
+// (outputs to the planes exchanged when swap_out: the last launch of an inverse)
 __device__ __forceinline__ void d_butterfly(double *yr, double *yi, size_t stride, int off, int k, int q,
-                                            double w_r, double w_i, double scale) {
+                                            double w_r, double w_i, double scale, bool swap_out = false) {
   double *r0 = yr + (size_t)(off + k) * stride, *i0 = yi + (size_t)(off + k) * stride;
   const size_t qs = (size_t)q * stride;
   const double u0r = r0[0], u1r = r0[qs], zpr = r0[2 * qs], zmr = r0[3 * qs];
@@ -189,6 +190,11 @@ __device__ __forceinline__ void d_butterfly(double *yr, double *yi, size_t strid
   const double pr = w_r * zpr + w_i * zpi, pi = w_r * zpi - w_i * zpr;
   const double mr = w_r * zmr - w_i * zmi, mi = w_r * zmi + w_i * zmr;
   const double sr = pr + mr, si = pi + mi, dr = pr - mr, di = pi - mi;
+  if (swap_out) {
+    double *t = r0;
+    r0 = i0;
+    i0 = t;
+  }
   r0[0] = (u0r + sr) * scale;
   r0[2 * qs] = (u0r - sr) * scale;
   r0[qs] = (u1r + di) * scale;
@@ -230,7 +236,7 @@ __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict_
                                                         int B, const SubRoot *__restrict__ roots, int nroots, int G,
                                                         SubSchedule big, SubSchedule small,
                                                         const double *__restrict__ wr, const double *__restrict__ wi,
-                                                        DConst K, double scale) {
+                                                        DConst K, double scale, int swap_in, int swap_out) {
   extern __shared__ double sm[];
   const int Tmax = big.size;
   const int lgT = 31 - __clz(Tmax);
@@ -272,8 +278,8 @@ __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict_
         int idx = rt.sn + j * rt.s;
         if (idx < 0) idx += N;
         const size_t b = (size_t)(b0 + g);
-        vr[u] = in[b * N + idx];
-        vi[u] = in[((size_t)B + b) * N + idx];
+        vr[u] = in[(swap_in ? (size_t)B + b : b) * N + idx];
+        vi[u] = in[(swap_in ? b : (size_t)B + b) * N + idx];
         dst[u] = g * istride + pidx(perm[j]);
       }
     }
@@ -325,8 +331,8 @@ __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict_
     if (!SINGLE && m >= T) continue;
     const int b = b0 + g;
     const double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
-    out[(size_t)b * N + rt.out + m] = yr[pidx(m)];
-    out[((size_t)B + b) * N + rt.out + m] = yi[pidx(m)];
+    out[(swap_out ? (size_t)B + b : (size_t)b) * N + rt.out + m] = yr[pidx(m)];
+    out[(swap_out ? (size_t)b : (size_t)B + b) * N + rt.out + m] = yi[pidx(m)];
   }
 }
 
@@ -335,7 +341,7 @@ __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict_
 __global__ void __launch_bounds__(256) d_level_kernel(double *__restrict__ y, int N, int B, int n,
                                                        const int *__restrict__ node_off, int nnodes,
                                                        const double *__restrict__ wr, const double *__restrict__ wi,
-                                                       double scale) {
+                                                       double scale, int swap_out) {
   const int q = n >> 2;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)nnodes * q * B) return;
@@ -344,7 +350,8 @@ __global__ void __launch_bounds__(256) d_level_kernel(double *__restrict__ y, in
   const int node = (int)(r % nnodes);
   const int b = (int)(r / nnodes);
   const int kn = k * (N / n);
-  d_butterfly(y + (size_t)b * N, y + ((size_t)B + b) * N, 1, node_off[node], k, q, wr[kn], wi[kn], scale);
+  d_butterfly(y + (size_t)b * N, y + ((size_t)B + b) * N, 1, node_off[node], k, q, wr[kn], wi[kn], scale,
+              swap_out != 0);
 }
 
 // Split step of the FP64 real transforms (n = 2M real points; layouts [c][b][k]).
@@ -429,7 +436,7 @@ static int d_sub_instances(const DDeviceTables &T) {
 }
 
 cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
-                            cudaStream_t s) {
+                            cudaStream_t s, bool swap_in, bool swap_out) {
   const DConst K{T.c8, T.c16a, T.c16b, T.c16c, T.c16d};
   const int size = T.sub[0].size;
   const int G = d_sub_instances(T);
@@ -444,10 +451,11 @@ cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *ou
   if (T.nroots == 1) {
     const int blocks = (B + G - 1) / G;
     d_sub_kernel<true><<<blocks, 256, smem, s>>>(in, out, T.N, B, T.roots, T.nroots, G, T.sub[0], T.sub[1], T.wr,
-                                                 T.wi, K, final_sub ? scale : 1.0);
+                                                 T.wi, K, final_sub ? scale : 1.0, swap_in, final_sub && swap_out);
   } else {
     d_sub_kernel<false><<<T.nroots * B, 256, smem, s>>>(in, out, T.N, B, T.roots, T.nroots, 1, T.sub[0], T.sub[1],
-                                                        T.wr, T.wi, K, final_sub ? scale : 1.0);
+                                                        T.wr, T.wi, K, final_sub ? scale : 1.0, swap_in,
+                                                        final_sub && swap_out);
   }
   for (int lv = 0; lv < T.upper.nlevels; ++lv) {
     const int threads = 256;
@@ -456,7 +464,8 @@ cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *ou
     const int lblocks = (int)((total + threads - 1) / threads);
     d_level_kernel<<<lblocks, threads, 0, s>>>(out, T.N, B, n, T.upper.node_off + T.upper.level_start[lv],
                                                T.upper.level_count[lv], T.wr, T.wi,
-                                               lv == T.upper.nlevels - 1 ? scale : 1.0);
+                                               lv == T.upper.nlevels - 1 ? scale : 1.0,
+                                               lv == T.upper.nlevels - 1 && swap_out);
   }
   return cudaGetLastError();
 }

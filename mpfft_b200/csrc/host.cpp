@@ -1211,12 +1211,16 @@ static int d_plan_init_nd(mpfft_d_plan *p, int rank, const unsigned long *dims) 
 // d_sr24_cp_fft in this order.  Scaling by 1/d per axis is exact.
 static cudaError_t d_transform(mpfft_d_plan *p, const double *in, double *out, int B, unsigned flags,
                                cudaStream_t st, double *tmp) {
-  if (p->rank == 1) return d_run_transform(p->tabs, in, out, B, d_scale(p, flags), st);
+  // MPFFT_INVERSE: the first launch reads the planes exchanged, the last writes
+  // them exchanged (transpositions keep planes apart), i.e. swap(FFT(swap(x)))
+  const bool inv = (flags & MPFFT_INVERSE) != 0;
+  if (p->rank == 1) return d_run_transform(p->tabs, in, out, B, d_scale(p, flags), st, inv, inv);
   const double *src = in;
   for (int s = p->rank - 1; s >= 0; --s) {
     const long long d = (long long)p->dims[s], R = (long long)p->N / d;
     const double sc = (flags & MPFFT_SCALED) ? 1.0 / (double)d : 1.0;
-    cudaError_t e = d_run_transform(p->axis[s]->tabs, src, tmp, (int)(B * R), sc, st);
+    cudaError_t e = d_run_transform(p->axis[s]->tabs, src, tmp, (int)(B * R), sc, st, inv && s == p->rank - 1,
+                                    inv && s == 0);
     if (e != cudaSuccess) return e;
     e = transpose_launch(reinterpret_cast<const uint32_t *>(tmp), reinterpret_cast<uint32_t *>(out), 2LL * B, R, d, 2,
                          st);

@@ -176,8 +176,10 @@ cudaError_t mp_export_launch(const uint32_t *planes, int N, int B, int L, const 
 cudaError_t transpose_launch(const uint32_t *in, uint32_t *out, long long nmat, long long R, long long C, int E,
                              cudaStream_t s);
 // FP64 layout: word (c, b, p) at base[(c*B + b)*N + p]  (signal-contiguous)
+// swap_in / swap_out: read the input's / write the output's real and imaginary
+// planes exchanged (both: the unscaled inverse, swap(FFT(swap(x))))
 cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
-                            cudaStream_t s);
+                            cudaStream_t s, bool swap_in = false, bool swap_out = false);
 // split step of the FP64 real transforms (n = 2M real points), d_kernels.cu
 cudaError_t d_real_split(bool forward, const double *in, double *out, int M, int B, const double *wc,
                          const double *ws, double scale, cudaStream_t s);
