@@ -192,6 +192,23 @@ int mpfft_mp_unpack(const mpfft_mp_plan *plan, unsigned long batch, const uint32
 
 /* FP64 plans.  Host arrays: signal b at [b*n, (b+1)*n) of each array. */
 int mpfft_d_plan_create(mpfft_d_plan **plan, unsigned long n);
+/* Double-double tier (about 106 bits; no counterpart in the reference): the
+ * same conjugate-pair split-radix transform with every value an unevaluated
+ * sum hi + lo of two doubles and every operation a compensated double-double
+ * one (error-free TwoSum / Fast2Sum / FMA TwoProd), twiddles rounded to
+ * double-double.  Normwise error against an exact DFT about log2(n) * 2^-104
+ * (tests bound it by 8 * log2(n) * 2^-104 against a 212-bit MPFR DFT).
+ * Host arrays: signal b at [b*n, (b+1)*n) of each of the eight arrays;
+ * flags MPFFT_SCALED (times 1/n, exact) and MPFFT_INVERSE.  Device layout:
+ * word (c, h, b, p) at base[((c*2 + h)*batch + b)*n + p], c = 0 real / 1
+ * imaginary, h = 0 high / 1 low part. */
+int mpfft_dd_plan_create(mpfft_d_plan **plan, unsigned long n);
+int mpfft_dd_execute(mpfft_d_plan *plan, unsigned long batch, const double *xr_hi, const double *xr_lo,
+                     const double *xi_hi, const double *xi_lo, double *yr_hi, double *yr_lo, double *yi_hi,
+                     double *yi_lo, unsigned flags);
+int mpfft_dd_execute_device(mpfft_d_plan *plan, unsigned long batch, const double *d_in, double *d_out,
+                            unsigned flags, void *stream);
+
 /* FP64 real transforms of n real points (n a power of two >= 2; no
  * counterpart in the reference): the n/2-point complex transform (the
  * reference's, bit-identical) plus one split step in double.  r2c: in[b*n + j]

@@ -73,6 +73,9 @@ def _load() -> C.CDLL:
         "mpfft_mp_plan_create_nd": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(ul), sl, C.c_uint]),
         "mpfft_d_plan_create_nd": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(ul)]),
         "mpfft_d_plan_create_real": (C.c_int, [C.POINTER(vp), ul]),
+        "mpfft_dd_plan_create": (C.c_int, [C.POINTER(vp), ul]),
+        "mpfft_dd_execute": (C.c_int, [vp, ul, dp, dp, dp, dp, dp, dp, dp, dp, C.c_uint]),
+        "mpfft_dd_execute_device": (C.c_int, [vp, ul, dp, dp, C.c_uint, vp]),
         "mpfft_d_execute_r2c": (C.c_int, [vp, ul, dp, dp, dp, C.c_uint]),
         "mpfft_d_execute_c2r": (C.c_int, [vp, ul, dp, dp, dp, C.c_uint]),
         "mpfft_mp_execute_r2c": (C.c_int, [vp, ul, vp, vp, vp, C.c_uint]),
@@ -333,6 +336,26 @@ class DRealPlan(DPlan):
 
     def c2r(self, batch, inr, ini, x, scaled=False) -> None:
         _check(lib.mpfft_d_execute_c2r(self.h, batch, _dp(inr), _dp(ini), _dp(x), SCALED if scaled else 0))
+
+
+class DDPlan(DPlan):
+    """Double-double (about 106-bit) plan for n points."""
+
+    def __init__(self, n: int):
+        h = C.c_void_p()
+        _check(lib.mpfft_dd_plan_create(C.byref(h), n))
+        self.h = h
+        self.n = n
+
+    def execute(self, batch, xr, xi, yr, yi, scaled=False, inverse=False) -> None:
+        """xr, xi, yr, yi: (hi, lo) pairs of float64 arrays."""
+        flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
+        _check(lib.mpfft_dd_execute(self.h, batch, _dp(xr[0]), _dp(xr[1]), _dp(xi[0]), _dp(xi[1]), _dp(yr[0]),
+                                    _dp(yr[1]), _dp(yi[0]), _dp(yi[1]), flags))
+
+    def execute_device(self, batch, d_in: int, d_out: int, scaled=False, stream: int = 0, inverse=False) -> None:
+        flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
+        _check(lib.mpfft_dd_execute_device(self.h, batch, d_in, d_out, flags, stream or None))
 
 
 class DPlanND(DPlan):

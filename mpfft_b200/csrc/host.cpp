@@ -481,6 +481,8 @@ struct mpfft_d_plan {
   std::unique_ptr<mpfft_d_plan> axis[3];
   double *d_tmp = nullptr;  // rank > 1: transposition buffer; real plans: split-step output
   size_t tmp_cap = 0;
+  bool dd = false;          // double-double tier (dd_kernels.cu)
+  double *d_wrl = nullptr, *d_wil = nullptr;
   bool real = false;        // real transform of n_real = 2N points: N-point complex transform + split step
   unsigned long n_real = 0;
   double *d_wc = nullptr, *d_ws = nullptr;  // real plans: cos, sin of 2 pi k / n_real, k < N/2
@@ -502,6 +504,8 @@ struct mpfft_d_plan {
     if (h_out) cudaFreeHost(h_out);
     if (d_tmp) cudaFree(d_tmp);
     if (d_wc) cudaFree(d_wc);
+    if (d_wrl) cudaFree(d_wrl);
+    if (d_wil) cudaFree(d_wil);
     if (d_ws) cudaFree(d_ws);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -1071,9 +1075,9 @@ static int upload(mpfft_d_plan *p, const std::vector<T> &v, const T **out) {
 
 // Schedule of a shared-memory sub-transform of `size` points: the leaves and
 // levels of its own recursion tree, and the DIT input order perm[m].
-static int build_sub(mpfft_d_plan *p, int size, SubSchedule &S) {
+static int build_sub(mpfft_d_plan *p, int size, SubSchedule &S, int leaf_max = 16) {
   HostTree t;
-  walk(t, size, 1, 0, 0, 16);
+  walk(t, size, 1, 0, 0, leaf_max);
   // invperm[j] = DIT position of element j of the sub-transform's input sequence
   std::vector<int> perm(size);
   for (const Leaf &lf : t.leaves)
@@ -1157,7 +1161,7 @@ static mpfft_d_plan *d_cached(unsigned long n) {
 }
 
 static int d_reserve(mpfft_d_plan *p, unsigned long batch) {
-  const size_t words = (size_t)2 * (p->real ? p->N + 1 : p->N) * batch;
+  const size_t words = (size_t)(p->dd ? 4 : 2) * (p->real ? p->N + 1 : p->N) * batch;
   if (words <= p->cap) return MPFFT_OK;
   if (p->d_in) cudaFree(p->d_in);
   if (p->d_out) cudaFree(p->d_out);
@@ -1276,6 +1280,72 @@ static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *in
   memcpy(outr, p->h_out, cim * sizeof(double));
   memcpy(outi, p->h_out + cim, cim * sizeof(double));
   return set_err(MPFFT_OK, "");
+}
+
+// Double-double plan: the same tree, cut at T = min(n, 2048) points, base cases
+// of at most 4 points, twiddles cos/sin(2 pi k/n) rounded to double-double.
+static int d_plan_init_dd(mpfft_d_plan *p, unsigned long n) {
+  if (!is_pow2(n)) return set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
+  if (n > (1UL << 26)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
+  if (int e = device_ready()) return e;
+  p->N = n;
+  p->dd = true;
+  p->tabs.N = (int)n;
+  const int T = (int)std::min<unsigned long>(n, kDDSubMax);
+  {
+    HostTree t;
+    walk(t, (int)n, 1, 0, 0, T);
+    std::vector<SubRoot> roots;
+    for (const Leaf &lf : t.leaves) roots.push_back(SubRoot{lf.sn, lf.s, lf.out, lf.n});
+    p->tabs.nroots = (int)roots.size();
+    if (int e = upload(p, roots, &p->tabs.roots)) return e;
+    if (int e = build_tree(p->upper, n, T)) return e;
+    p->tabs.upper = p->upper.tabs;
+  }
+  if (int e = build_sub(p, T, p->tabs.sub[0], 4)) return e;
+  if (T >= 2) {
+    if (int e = build_sub(p, T / 2, p->tabs.sub[1], 4)) return e;
+  } else {
+    p->tabs.sub[1] = p->tabs.sub[0];
+  }
+  const unsigned long q = std::max<unsigned long>(1, n / 4);
+  std::vector<double> ch(q), cl(q), sh(q), sl(q);
+  parallel_for((long)q, 64, [&](long a, long b) {
+    mpfr_t th, c, s, r;
+    mpfr_init2(th, 200);
+    mpfr_init2(c, 160);
+    mpfr_init2(s, 160);
+    mpfr_init2(r, 160);
+    for (long k = a; k < b; ++k) {
+      mpfr_const_pi(th, MPFR_RNDN);
+      mpfr_mul_ui(th, th, 2UL * (unsigned long)k, MPFR_RNDN);
+      mpfr_div_ui(th, th, n, MPFR_RNDN);
+      mpfr_sin_cos(s, c, th, MPFR_RNDN);
+      ch[k] = mpfr_get_d(c, MPFR_RNDN);
+      mpfr_sub_d(r, c, ch[k], MPFR_RNDN);
+      cl[k] = mpfr_get_d(r, MPFR_RNDN);
+      sh[k] = mpfr_get_d(s, MPFR_RNDN);
+      mpfr_sub_d(r, s, sh[k], MPFR_RNDN);
+      sl[k] = mpfr_get_d(r, MPFR_RNDN);
+    }
+    mpfr_clear(th);
+    mpfr_clear(c);
+    mpfr_clear(s);
+    mpfr_clear(r);
+    mpfr_free_cache();
+  });
+  double **dst[4] = {&p->d_wr, &p->d_wrl, &p->d_wi, &p->d_wil};
+  const std::vector<double> *src[4] = {&ch, &cl, &sh, &sl};
+  for (int i = 0; i < 4; ++i) {
+    CUDA_TRY(cudaMalloc(dst[i], q * sizeof(double)));
+    CUDA_TRY(cudaMemcpy(*dst[i], src[i]->data(), q * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  p->tabs.wr = p->d_wr;
+  p->tabs.wrl = p->d_wrl;
+  p->tabs.wi = p->d_wi;
+  p->tabs.wil = p->d_wil;
+  CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  return MPFFT_OK;
 }
 
 // real transform of n >= 2 points: the n/2-point complex plan plus split twiddles
@@ -1579,6 +1649,61 @@ MPFFT_API int mpfft_d_plan_create(mpfft_d_plan **plan, unsigned long n) {
   return set_err(MPFFT_OK, "");
 }
 
+MPFFT_API int mpfft_dd_plan_create(mpfft_d_plan **plan, unsigned long n) {
+  if (!plan) return set_err(MPFFT_EINVAL, "NULL plan pointer");
+  *plan = nullptr;
+  std::unique_ptr<mpfft_d_plan> p(new (std::nothrow) mpfft_d_plan);
+  if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
+  if (int e = d_plan_init_dd(p.get(), n)) return e;
+  *plan = p.release();
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_dd_execute(mpfft_d_plan *plan, unsigned long batch, const double *xr_hi, const double *xr_lo,
+                               const double *xi_hi, const double *xi_lo, double *yr_hi, double *yr_lo,
+                               double *yi_hi, double *yi_lo, unsigned flags) {
+  if (!plan || !xr_hi || !xr_lo || !xi_hi || !xi_lo || !yr_hi || !yr_lo || !yi_hi || !yi_lo)
+    return set_err(MPFFT_EINVAL, "NULL argument");
+  if (!plan->dd) return set_err(MPFFT_EINVAL, "not a double-double plan (mpfft_dd_plan_create)");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  if ((unsigned long long)batch * plan->N > (unsigned long long)INT32_MAX)
+    return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  if (flags & MPFFT_INVERSE) {  // ifft(X) = swap(FFT(swap(X))) (times 1/n if scaled)
+    std::swap(xr_hi, xi_hi);
+    std::swap(xr_lo, xi_lo);
+    std::swap(yr_hi, yi_hi);
+    std::swap(yr_lo, yi_lo);
+  }
+  std::lock_guard<std::mutex> g(plan->mu);
+  if (int e = d_reserve(plan, batch)) return e;
+  const size_t pl = (size_t)plan->N * batch;
+  const double *src[4] = {xr_hi, xr_lo, xi_hi, xi_lo};
+  for (int i = 0; i < 4; ++i) memcpy(plan->h_in + i * pl, src[i], pl * sizeof(double));
+  CUDA_TRY(cudaMemcpyAsync(plan->d_in, plan->h_in, 4 * pl * sizeof(double), cudaMemcpyHostToDevice, plan->stream));
+  CUDA_TRY(dd_run_transform(plan->tabs, plan->d_in, plan->d_out, (int)batch, d_scale(plan, flags), plan->stream));
+  CUDA_TRY(cudaMemcpyAsync(plan->h_out, plan->d_out, 4 * pl * sizeof(double), cudaMemcpyDeviceToHost, plan->stream));
+  CUDA_TRY(cudaStreamSynchronize(plan->stream));
+  double *dst[4] = {yr_hi, yr_lo, yi_hi, yi_lo};
+  for (int i = 0; i < 4; ++i) memcpy(dst[i], plan->h_out + i * pl, pl * sizeof(double));
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_dd_execute_device(mpfft_d_plan *plan, unsigned long batch, const double *d_in, double *d_out,
+                                      unsigned flags, void *stream) {
+  if (!plan || !d_in || !d_out) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (!plan->dd) return set_err(MPFFT_EINVAL, "not a double-double plan (mpfft_dd_plan_create)");
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  if ((unsigned long long)batch * plan->N > (unsigned long long)INT32_MAX)
+    return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  const size_t bytes = (size_t)4 * plan->N * batch * 8;
+  const char *a = (const char *)d_in, *b = (const char *)d_out;
+  if (a < b + bytes && b < a + bytes) return set_err(MPFFT_EINVAL, "input and output buffers overlap");
+  const bool inv = (flags & MPFFT_INVERSE) != 0;
+  CUDA_TRY(dd_run_transform(plan->tabs, d_in, d_out, (int)batch, d_scale(plan, flags), (cudaStream_t)stream, inv,
+                            inv));
+  return set_err(MPFFT_OK, "");
+}
+
 MPFFT_API int mpfft_d_plan_create_real(mpfft_d_plan **plan, unsigned long n) {
   if (!plan) return set_err(MPFFT_EINVAL, "NULL plan pointer");
   *plan = nullptr;
@@ -1624,6 +1749,7 @@ MPFFT_API int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const dou
                               double *outr, double *outi, unsigned flags) {
   if (!plan || !inr || !ini || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
   if (plan->real) return set_err(MPFFT_EINVAL, "real plan: use mpfft_d_execute_r2c / mpfft_d_execute_c2r");
+  if (plan->dd) return set_err(MPFFT_EINVAL, "double-double plan: use mpfft_dd_execute");
   if (batch == 0) return set_err(MPFFT_OK, "");
   if (flags & MPFFT_INVERSE) {  // ifft(X) = swap(FFT(swap(X))) (times 1/n if scaled)
     std::swap(inr, ini);
@@ -1637,6 +1763,7 @@ MPFFT_API int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, co
                                      unsigned flags, void *stream) {
   if (!plan || !d_in || !d_out) return set_err(MPFFT_EINVAL, "NULL argument");
   if (plan->real) return set_err(MPFFT_EINVAL, "real plans have no device-layout entry point");
+  if (plan->dd) return set_err(MPFFT_EINVAL, "double-double plan: use mpfft_dd_execute_device");
   if (batch == 0) return set_err(MPFFT_OK, "");
   const size_t bytes = (size_t)2 * plan->N * batch * 8;
   const char *a = (const char *)d_in, *b = (const char *)d_out;

@@ -71,6 +71,7 @@ struct DDeviceTables {
   int N = 0;
   const double *wr = nullptr;  // [N/4] cos(2 pi k/N)
   const double *wi = nullptr;  // [N/4] sin(2 pi k/N)
+  const double *wrl = nullptr, *wil = nullptr;  // double-double plans: low parts of wr, wi
   double c8 = 0, c16a = 0, c16b = 0, c16c = 0, c16d = 0;
   // shared-memory sub-transforms (sizes T and T/2) ...
   int nroots = 0;
@@ -82,6 +83,7 @@ struct DDeviceTables {
 
 constexpr int kMaxDevices = 64;
 constexpr int kDSubMax = 4096;  // FP64: largest shared-memory sub-transform (64 KB)
+constexpr int kDDSubMax = 2048; // double-double: largest shared-memory sub-transform (64 KB)
 
 // What the static-scratch entry point needs to know about a plan.
 struct MpPlanView {
@@ -180,6 +182,9 @@ cudaError_t transpose_launch(const uint32_t *in, uint32_t *out, long long nmat, 
 // planes exchanged (both: the unscaled inverse, swap(FFT(swap(x))))
 cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
                             cudaStream_t s, bool swap_in = false, bool swap_out = false);
+// double-double tier (dd_kernels.cu); layout word (c, h, b, p) at ((c*2 + h)*B + b)*N + p
+cudaError_t dd_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
+                             cudaStream_t s, bool swap_in = false, bool swap_out = false);
 // split step of the FP64 real transforms (n = 2M real points), d_kernels.cu
 cudaError_t d_real_split(bool forward, const double *in, double *out, int M, int B, const double *wc,
                          const double *ws, double scale, cudaStream_t s);

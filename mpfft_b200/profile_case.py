@@ -56,13 +56,39 @@ def run_fp64(a) -> None:
           f"in+out {nbytes / ms / 1e6:.0f} GB/s")
 
 
+def run_dd(a) -> None:
+    """Double-double tier: layout [c][h][b][p]; time per batch and in+out bytes / time."""
+    import torch
+
+    import mpfft_b200 as M
+
+    plan = M.DDPlan(a.n)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    hi = torch.rand((2, a.batch, a.n), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    d_in = torch.stack((hi[0], hi[0] * 2.0 ** -60, hi[1], hi[1] * 2.0 ** -60)).contiguous()
+    d_out = torch.empty_like(d_in)
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        plan.execute_device(a.batch, d_in.data_ptr(), d_out.data_ptr(), stream=s.cuda_stream)
+    e0.record(s)
+    for _ in range(a.reps):
+        plan.execute_device(a.batch, d_in.data_ptr(), d_out.data_ptr(), stream=s.cuda_stream)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.reps
+    nbytes = 2 * d_in.numel() * 8
+    print(f"dd n={a.n} batch={a.batch}: {ms:.4f} ms per batch, {a.batch / ms * 1e3:.0f} FFT/s, "
+          f"in+out {nbytes / ms / 1e6:.0f} GB/s")
+
+
 def main():
     import torch
 
     import mpfft_b200 as M
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--tier", default="mp", choices=["mp", "fp64"])
+    ap.add_argument("--tier", default="mp", choices=["mp", "fp64", "dd"])
     ap.add_argument("--n", type=int, default=1024)
     ap.add_argument("--prec", type=int, default=1024)
     ap.add_argument("--batch", type=int, default=512)
@@ -72,6 +98,9 @@ def main():
     a = ap.parse_args()
     if a.tier == "fp64":
         run_fp64(a)
+        return
+    if a.tier == "dd":
+        run_dd(a)
         return
     plan = M.MpPlan(a.n, a.prec, tensor="force" if a.force_tensor else not a.no_tensor)
     host = synthetic_planes(a.n, plan.limbs, plan.frac_bits, a.batch)

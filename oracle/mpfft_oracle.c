@@ -102,6 +102,26 @@ OAPI void orc_mp_hermitian_extend(unsigned long n, mpfr_t *hr, mpfr_t *hi, mpfr_
   }
 }
 
+/* double-double views: hi[k] = a[k] rounded to double, lo[k] = (a[k] - hi[k])
+ * rounded; set: a[k] = hi[k] + lo[k] (rounded to a's precision) */
+OAPI void orc_mp_get_dd(mpfr_t *a, double *hi, double *lo, unsigned long n) {
+  mpfr_t r;
+  mpfr_init2(r, mpfr_get_prec(a[0]) + 64);
+  for (unsigned long k = 0; k < n; k++) {
+    hi[k] = mpfr_get_d(a[k], RN);
+    mpfr_sub_d(r, a[k], hi[k], RN);
+    lo[k] = mpfr_get_d(r, RN);
+  }
+  mpfr_clear(r);
+}
+
+OAPI void orc_mp_set_dd(mpfr_t *a, const double *hi, const double *lo, unsigned long n) {
+  for (unsigned long k = 0; k < n; k++) {
+    mpfr_set_d(a[k], hi[k], RN);
+    mpfr_add_d(a[k], a[k], lo[k], RN);
+  }
+}
+
 OAPI void orc_mp_set_nan(mpfr_t *a, unsigned long k) { mpfr_set_nan(a[k]); }
 OAPI void orc_mp_set_inf(mpfr_t *a, unsigned long k, int sign) { mpfr_set_inf(a[k], sign); }
 

@@ -109,6 +109,8 @@ void mpfr_set_zero(mpfr_ptr, int);
 void mpfr_set_nan(mpfr_ptr);
 void mpfr_set_inf(mpfr_ptr, int);
 double mpfr_get_d(mpfr_srcptr, mpfr_rnd_t);
+int mpfr_sub_d(mpfr_ptr, mpfr_srcptr, double, mpfr_rnd_t);
+int mpfr_add_d(mpfr_ptr, mpfr_srcptr, double, mpfr_rnd_t);
 double mpfr_get_d_2exp(long *, mpfr_srcptr, mpfr_rnd_t);
 mpfr_exp_t mpfr_get_exp(mpfr_srcptr);
 char *mpfr_get_str(char *, mpfr_exp_t *, int, size_t, mpfr_srcptr, mpfr_rnd_t);

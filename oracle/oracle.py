@@ -70,6 +70,8 @@ def lib() -> C.CDLL:
         "orc_mp_dft": (None, [ul, sl, vp, vp, vp, vp]),
         "orc_mp_hermitian_extend": (None, [ul, vp, vp, vp, vp]),
         "orc_mp_dft_nd": (None, [C.c_int, C.POINTER(C.c_ulong), sl, vp, vp, vp, vp]),
+        "orc_mp_get_dd": (None, [vp, vp, vp, ul]),
+        "orc_mp_set_dd": (None, [vp, vp, vp, ul]),
         "orc_mp_errors": (None, [ul, vp, vp, vp, vp, dp]),
         "orc_d_new": (vp, [ul]),
         "orc_d_delete": (None, [vp]),
