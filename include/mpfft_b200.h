@@ -159,6 +159,17 @@ int mpfft_mp_execute(mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr
 int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, const uint32_t *d_in, uint32_t *d_out,
                             void *stream);
 
+/* Uneven batch (no counterpart in the reference): `count` signals of
+ * different lengths n[i] (powers of two) and precisions; signal i occupies
+ * inr[i][0..n[i]) etc., working precision the largest of its four arrays'
+ * first elements.  Signals with the same length and limb count run as one
+ * batched execution of a cached plan (GPU conversion pipeline included), so
+ * each result is identical to a single call of the drop-in.  flags:
+ * MPFFT_SCALED, MPFFT_INVERSE.  On error the failing groups' outputs are
+ * NaN. */
+int mpfft_mp_execute_mixed(unsigned long count, const unsigned long *n, mpfr_t *const *inr, mpfr_t *const *ini,
+                           mpfr_t *const *outr, mpfr_t *const *outi, unsigned flags);
+
 /* Real transforms (no counterpart in the reference, whose README lists
  * "only complex input"; a real signal there is a complex one with zero
  * imaginary parts).  A real plan for n real points (n a power of two, n >= 2)

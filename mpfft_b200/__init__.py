@@ -71,6 +71,8 @@ def _load() -> C.CDLL:
         "mpfft_mp_execute_device": (C.c_int, [vp, ul, u32p, u32p, vp]),
         "mpfft_mp_plan_create_real": (C.c_int, [C.POINTER(vp), ul, sl, C.c_uint]),
         "mpfft_mp_plan_create_nd": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(ul), sl, C.c_uint]),
+        "mpfft_mp_execute_mixed": (C.c_int, [ul, C.POINTER(ul), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                             C.POINTER(vp), C.c_uint]),
         "mpfft_d_plan_create_nd": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(ul)]),
         "mpfft_d_plan_create_real": (C.c_int, [C.POINTER(vp), ul]),
         "mpfft_dd_plan_create": (C.c_int, [C.POINTER(vp), ul]),
@@ -278,6 +280,15 @@ class MpRealPlan:
 
     def c2r(self, batch, inr, ini, x, scaled=False) -> None:
         _check(lib.mpfft_mp_execute_c2r(self.h, batch, inr, ini, x, SCALED if scaled else 0))
+
+
+def mp_execute_mixed(ns, inr, ini, outr, outi, scaled=False, inverse=False) -> None:
+    """Uneven batch: lists of lengths and of mpfr_t array addresses per signal."""
+    k = len(ns)
+    arr = lambda v, t: (t * k)(*v)
+    flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
+    _check(lib.mpfft_mp_execute_mixed(k, arr(ns, C.c_ulong), arr(inr, C.c_void_p), arr(ini, C.c_void_p),
+                                      arr(outr, C.c_void_p), arr(outi, C.c_void_p), flags))
 
 
 def tc_mul(limbs: int, batch: int, d_x: int, d_w: int, d_out: int, stream: int = 0) -> None:

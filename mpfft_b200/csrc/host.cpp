@@ -623,11 +623,16 @@ static int mp_reserve(mpfft_mp_plan *p, unsigned long batch) {
 }
 
 // Geometry of a host mpfr_t array: element q < n of signal b is a[b*pitch + q*s].
+// With per-signal bases (base[part] non-null) element q of signal b is
+// base[part][b][q*s] instead (part 0 real, 1 imaginary), and the array
+// arguments are ignored.
 struct IoShape {
   unsigned long n, pitch, s;
+  mpfr_t *const *base[2] = {nullptr, nullptr};
 };
 static inline IoShape io_signals(unsigned long n, unsigned long s) { return IoShape{n, n * s, s}; }
-static inline mpfr_ptr elem(mpfr_t *a, unsigned long b, const IoShape &io, unsigned long q) {
+static inline mpfr_ptr elem(mpfr_t *a, int part, unsigned long b, const IoShape &io, unsigned long q) {
+  if (io.base[part]) return io.base[part][b][q * io.s];
   return a[b * io.pitch + q * io.s];
 }
 
@@ -645,7 +650,7 @@ static int mp_pack_impl(const mpfft_mp_plan *P, unsigned long batch, const IoSha
       long e_s = LONG_MIN;
       for (unsigned long p = 0; p < N; ++p) {
         for (int c = 0; c < 2; ++c) {
-          mpfr_srcptr x = elem(c ? ini : inr, b, io, p);
+          mpfr_srcptr x = elem(c ? ini : inr, c, b, io, p);
           if (!mpfr_number_p(x)) bad[b] = 1;
           else if (!mpfr_zero_p(x) && x->_mpfr_exp > e_s) e_s = x->_mpfr_exp;
         }
@@ -661,7 +666,7 @@ static int mp_pack_impl(const mpfft_mp_plan *P, unsigned long batch, const IoSha
     for (long t = a0; t < a1; ++t) {
       const unsigned long p = t / batch, b = t % batch;
       for (int c = 0; c < 2; ++c) {
-        uint32_t sg = mpfr_to_fixed(elem(c ? ini : inr, b, io, p), L, P->F, exps[b], tmp);
+        uint32_t sg = mpfr_to_fixed(elem(c ? ini : inr, c, b, io, p), L, P->F, exps[b], tmp);
         if (sg) {  // two's complement
           uint32_t cy = 1;
           for (int i = 0; i < L; ++i) {
@@ -691,7 +696,7 @@ static void mp_unpack_impl(const mpfft_mp_plan *P, unsigned long batch, const ui
       for (int c = 0; c < 2; ++c) {
         const uint32_t *src = planes + (size_t)c * L * plane + (size_t)p * batch + b;
         for (int i = 0; i < L; ++i) tmp[i] = src[(size_t)i * plane];
-        fixed_to_mpfr(tmp, L, exps[b] - P->F - fadj, elem(c ? outi : outr, b, io, p));
+        fixed_to_mpfr(tmp, L, exps[b] - P->F - fadj, elem(c ? outi : outr, c, b, io, p));
       }
     }
   });
@@ -805,17 +810,18 @@ static cudaError_t mp_device_pipeline(const mpfft_mp_plan *p, int mode, uint32_t
 static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, const IoShape &ii, mpfr_t *inr,
                               mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj) {
   const unsigned long Ni = ii.n, No = oo.n;
-  const long prec_out = mpfr_get_prec(outr[0]);
-  const int nli = nlimbs64(mpfr_get_prec(inr[0])), nlo = nlimbs64(prec_out);
+  const long prec_out = mpfr_get_prec(elem(outr, 0, 0, oo, 0));
+  const int nli = nlimbs64(mpfr_get_prec(elem(inr, 0, 0, ii, 0))), nlo = nlimbs64(prec_out);
   std::vector<int> bad(batch, 0);
   parallel_for((long)batch, 1, [&](long b0, long b1) {
     for (long b = b0; b < b1; ++b) {
       for (unsigned long q = 0; q < Ni && !bad[b]; ++q) {
-        mpfr_srcptr a = elem(inr, b, ii, q), c = elem(ini, b, ii, q);
+        mpfr_srcptr a = elem(inr, 0, b, ii, q), c = elem(ini, 1, b, ii, q);
         if (nlimbs64(a->_mpfr_prec) != nli || nlimbs64(c->_mpfr_prec) != nli) bad[b] = 1;
       }
       for (unsigned long q = 0; q < No && !bad[b]; ++q)
-        if (elem(outr, b, oo, q)->_mpfr_prec != prec_out || elem(outi, b, oo, q)->_mpfr_prec != prec_out) bad[b] = 1;
+        if (elem(outr, 0, b, oo, q)->_mpfr_prec != prec_out || elem(outi, 1, b, oo, q)->_mpfr_prec != prec_out)
+          bad[b] = 1;
     }
   });
   for (unsigned long b = 0; b < batch; ++b)
@@ -841,7 +847,7 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
       constexpr long kAhead = 8;  // significands prefetched ahead of use
       auto at = [&](long u) {
         const long bb = u / (2 * (long)Ni), part = (u / (long)Ni) & 1;
-        return elem(part ? ini : inr, b0 + bb, ii, (unsigned long)(u % (long)Ni));
+        return elem(part ? ini : inr, (int)part, b0 + bb, ii, (unsigned long)(u % (long)Ni));
       };
       for (long u = x0; u < std::min(x1, x0 + kAhead); ++u) __builtin_prefetch(at(u)->_mpfr_d);
       for (long u = x0; u < x1; ++u) {
@@ -892,7 +898,7 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
       constexpr long kAhead = 8;  // destination significands prefetched ahead of use
       auto at = [&](long u) {
         const long bb = u / (2 * (long)No), part = (u / (long)No) & 1;
-        return elem(part ? outi : outr, b0 + bb, oo, (unsigned long)(u % (long)No));
+        return elem(part ? outi : outr, (int)part, b0 + bb, oo, (unsigned long)(u % (long)No));
       };
       for (long u = x0; u < std::min(x1, x0 + kAhead); ++u) __builtin_prefetch(at(u)->_mpfr_d, 1);
       for (long u = x0; u < x1; ++u) {
@@ -1558,6 +1564,64 @@ MPFFT_API int mpfft_mp_execute(mpfft_mp_plan *plan, unsigned long batch, mpfr_t 
     mp_fill_nan(outi, plan->N * batch);
   }
   return e;
+}
+
+MPFFT_API int mpfft_mp_execute_mixed(unsigned long count, const unsigned long *n, mpfr_t *const *inr,
+                                     mpfr_t *const *ini, mpfr_t *const *outr, mpfr_t *const *outi, unsigned flags) {
+  if (!n || !inr || !ini || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (flags & MPFFT_INVERSE) {  // ifft(X) = swap(FFT(swap(X))) (times 1/n if scaled)
+    std::swap(inr, ini);
+    std::swap(outr, outi);
+    flags &= ~MPFFT_INVERSE;
+  }
+  // group the signals by (length, limb count): each group is one batched execution of a cached plan
+  std::map<std::pair<unsigned long, int>, std::vector<unsigned long>> groups;
+  std::vector<long> prec(count);
+  for (unsigned long i = 0; i < count; ++i) {
+    if (!inr[i] || !ini[i] || !outr[i] || !outi[i]) return set_err(MPFFT_EINVAL, "NULL array of signal %lu", i);
+    if (!is_pow2(n[i])) return set_err(MPFFT_EINVAL, "n[%lu]=%lu is not a power of two", i, n[i]);
+    prec[i] = mp_call_prec(inr[i], ini[i], outr[i], outi[i]);
+    if (prec[i] < 2) return set_err(MPFFT_EINVAL, "signal %lu: precision %ld < 2", i, prec[i]);
+    groups[std::make_pair(n[i], mp_limbs_for(n[i], prec[i]))].push_back(i);
+  }
+  int first_err = MPFFT_OK;
+  std::string first_msg;
+  for (auto &kv : groups) {
+    const unsigned long nn = kv.first.first;
+    const std::vector<unsigned long> &ids = kv.second;
+    long pg = 2;
+    for (unsigned long i : ids) pg = std::max(pg, prec[i]);
+    mpfft_mp_plan *p = mp_cached(nn, pg);
+    int e = p ? MPFFT_OK : g_err;
+    if (e == MPFFT_OK) {
+      std::vector<mpfr_t *> bi[2], bo[2];
+      for (unsigned long i : ids) {
+        bi[0].push_back(inr[i]);
+        bi[1].push_back(ini[i]);
+        bo[0].push_back(outr[i]);
+        bo[1].push_back(outi[i]);
+      }
+      IoShape ii = io_signals(nn, 1), oo = io_signals(nn, 1);
+      ii.base[0] = bi[0].data();
+      ii.base[1] = bi[1].data();
+      oo.base[0] = bo[0].data();
+      oo.base[1] = bo[1].data();
+      const long shift = (flags & MPFFT_SCALED) ? ilog2(nn) : 0;
+      e = mp_execute_impl(p, ids.size(), kComplex, ii, nullptr, nullptr, oo, nullptr, nullptr, shift);
+    }
+    if (e != MPFFT_OK) {
+      if (first_err == MPFFT_OK) {
+        first_err = e;
+        first_msg = g_msg;
+      }
+      for (unsigned long i : ids) {
+        mp_fill_nan(outr[i], nn);
+        mp_fill_nan(outi[i], nn);
+      }
+    }
+  }
+  if (first_err != MPFFT_OK) return set_err(first_err, "%s", first_msg.c_str());
+  return set_err(MPFFT_OK, "");
 }
 
 MPFFT_API int mpfft_mp_plan_create_real(mpfft_mp_plan **plan, unsigned long n, long prec, unsigned flags) {

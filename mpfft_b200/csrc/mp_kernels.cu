@@ -279,7 +279,8 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
 cudaError_t mp_run_transform(int L, const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
                              cudaStream_t s, float *launch_ms, uint32_t *big_scratch) {
   if (L > kMaxLimbs || mp_tc_used(T, L)) {
-    if (!big_scratch || L > kMaxLimbsBig) return cudaErrorInvalidValue;
+    // transforms without butterfly levels (N <= 4) need no scratch
+    if ((!big_scratch && T.nlevels > 0) || L > kMaxLimbsBig) return cudaErrorInvalidValue;
     return mp_big_run_transform(L, T, in, out, B, big_scratch, s, launch_ms);
   }
   switch (L) {

@@ -255,7 +255,8 @@ def test_mp_inverse_entry(M, orc, n, p):
     assert L.orc_mp_count_diff(wr.ptr, yr.ptr, n) == 0 and L.orc_mp_count_diff(wi.ptr, yi.ptr, n) == 0
 
 
-@pytest.mark.parametrize("n,p,batch", [(16, 2048, 1), (64, 2048, 32), (16, 4096, 2), (8, 8192, 1), (256, 1100, 1)])
+@pytest.mark.parametrize("n,p,batch", [(16, 2048, 1), (64, 2048, 32), (16, 4096, 2), (8, 8192, 1), (256, 1100, 1),
+                                     (1, 1100, 3), (2, 2048, 1), (4, 9000, 2)])
 def test_mp_large_precision(M, orc, n, p, batch):
     """Precisions beyond the register kernels (L > 34 limbs) run the streaming
     kernels: same error bound against the 2P-bit DFT, no worse than the
