@@ -154,8 +154,17 @@ __device__ __forceinline__ void combine(uint32_t *u0, uint32_t *u1, uint32_t *zp
 //   k = q/2  P=(Zr+-Zi)c      m.i = (Zi-Zr)c | (Zr+Zi)c    m.r = P -> im slot
 //                                   -> re slot
 // so m.r ends in the imaginary slot and m.i in the real slot ("swapped").
+// CTAs per SM the register allocation must allow: more warps hide more
+// latency while the product still fits without spills (measured at N=1024,
+// batch 2048: 13 limbs +15 % with 6 instead of 4, 17 limbs +8.5 % with 5;
+// from 20 limbs up the smaller allocation spills).
 template <int L>
-__global__ void __launch_bounds__(128, 4) mp_level_kernel(uint32_t *__restrict__ y, int N, int B, int n,
+constexpr int level_min_blocks() {
+  return L <= 14 ? 6 : (L <= 19 ? 5 : 4);
+}
+
+template <int L>
+__global__ void __launch_bounds__(128, level_min_blocks<L>()) mp_level_kernel(uint32_t *__restrict__ y, int N, int B, int n,
                                                           const int *__restrict__ node_off, int nnodes,
                                                           const uint32_t *__restrict__ tw,
                                                           const uint8_t *__restrict__ dneg, int tws) {
