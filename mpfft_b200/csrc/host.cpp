@@ -801,31 +801,25 @@ static cudaError_t mp_device_pipeline(const mpfft_mp_plan *p, int mode, uint32_t
   return mp_run_transform(p->L, p->tabs, b, a, B, st, nullptr, big);
 }
 
-// All inputs with one limb count and all outputs with one precision: the
-// conversion runs on the GPU and the host only moves raw significand limbs.
-// The batch is processed in chunks through two slots (stream + staging each):
-// while the GPU copies and transforms chunk i, the host scatters chunk i-1's
-// results and gathers chunk i+1's inputs.  Returns -1 when the call does not
-// qualify (mixed precisions).  fadj: output value = A * 2^(e_s - F - fadj).
+// Signals whose inputs share one limb count and whose outputs share one
+// precision (those of signal 0): the conversion runs on the GPU and the host
+// only moves raw significand limbs.  The batch is processed in chunks through
+// two slots (stream + staging each): while the GPU copies and transforms chunk
+// i, the host scatters chunk i-1's results and gathers chunk i+1's inputs.
+// The precisions are checked chunk by chunk as the pipeline reaches them (the
+// inputs' inside the gather, which reads the same mpfr_t fields anyway; the
+// outputs' just before it), not in a separate pass over the whole batch.  At
+// the first chunk that holds a different precision the pipeline drains and
+// stops: *done = the number of leading signals it completed, all of them with
+// their outputs written; the caller converts the rest on the host.
+// fadj: output value = A * 2^(e_s - F - fadj).
 static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, const IoShape &ii, mpfr_t *inr,
-                              mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj) {
+                              mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj,
+                              unsigned long *done) {
+  *done = 0;
   const unsigned long Ni = ii.n, No = oo.n;
   const long prec_out = mpfr_get_prec(elem(outr, 0, 0, oo, 0));
   const int nli = nlimbs64(mpfr_get_prec(elem(inr, 0, 0, ii, 0))), nlo = nlimbs64(prec_out);
-  std::vector<int> bad(batch, 0);
-  parallel_for((long)batch, 1, [&](long b0, long b1) {
-    for (long b = b0; b < b1; ++b) {
-      for (unsigned long q = 0; q < Ni && !bad[b]; ++q) {
-        mpfr_srcptr a = elem(inr, 0, b, ii, q), c = elem(ini, 1, b, ii, q);
-        if (nlimbs64(a->_mpfr_prec) != nli || nlimbs64(c->_mpfr_prec) != nli) bad[b] = 1;
-      }
-      for (unsigned long q = 0; q < No && !bad[b]; ++q)
-        if (elem(outr, 0, b, oo, q)->_mpfr_prec != prec_out || elem(outi, 1, b, oo, q)->_mpfr_prec != prec_out)
-          bad[b] = 1;
-    }
-  });
-  for (unsigned long b = 0; b < batch; ++b)
-    if (bad[b]) return -1;
   // chunks of up to 256 signals (a multiple of 32 keeps every warp on one
   // butterfly), and at most ~256 MiB of staging per slot
   const size_t per_signal = (size_t)2 * p->pts_max() * ((nli + nlo) * 8 + 2 * 4 * p->L + 18);
@@ -836,10 +830,27 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
   if (int e = mp_conv_reserve(p, chunk, nli, nlo)) return e;
   const unsigned long nchunks = (batch + chunk - 1) / chunk;
   const long emin = mpfr_get_emin(), emax = mpfr_get_emax();
-  std::vector<int> nonfin(nchunks, 0);
+  std::vector<int> nonfin(nchunks, 0), mixed(nchunks, 0);
 
+  // outputs of chunk ci all at prec_out (checked before any input of the chunk
+  // is staged, so a chunk is either converted whole here or not at all)
+  auto outputs_uniform = [&](unsigned long ci) {
+    const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
+    std::atomic<int> bad{0};
+    parallel_for((long)(2 * cb * No), 4096, [&](long x0, long x1) {
+      for (long u = x0; u < x1; ++u) {
+        const long bb = u / (2 * (long)No), part = (u / (long)No) & 1;
+        if (elem(part ? outi : outr, (int)part, b0 + bb, oo, (unsigned long)(u % (long)No))->_mpfr_prec != prec_out) {
+          bad.store(1, std::memory_order_relaxed);
+          return;
+        }
+      }
+    });
+    return bad.load() == 0;
+  };
   // staging is signal-major: component u = (signal*2 + part)*Ni + q, the order
-  // the host walks the mpfr_t arrays in, so both sides stream
+  // the host walks the mpfr_t arrays in, so both sides stream.  An input with
+  // another limb count marks the chunk mixed; its significand is not read.
   auto gather = [&](unsigned long ci) {
     auto &c = p->cv[ci & 1];
     const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
@@ -857,6 +868,10 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
           __builtin_prefetch(d + nli - 1);
         }
         mpfr_srcptr x = at(u);
+        if (nlimbs64(x->_mpfr_prec) != nli) {
+          mixed[ci] = 1;
+          break;
+        }
         if (x->_mpfr_exp <= LONG_MIN + 3) {  // MPFR's reserved exponents: zero, NaN, infinity
           if (!mpfr_zero_p(x)) nonfin[ci] = 1;
           stage_word(c.h_ei + u, INT64_MIN);
@@ -928,23 +943,29 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
     return MPFFT_OK;
   };
 
-  // validate every input before any output is written
+  // chunks [0, scattered) have their outputs written
+  unsigned long scattered = 0;
+  auto drain = [&](unsigned long upto) -> int {
+    for (; scattered < upto; ++scattered)
+      if (int e = scatter(scattered)) return e;
+    return MPFFT_OK;
+  };
   int err = MPFFT_OK;
-  gather(0);
-  if (nonfin[0]) return set_err(MPFFT_ENONFINITE, "input holds NaN or infinity");
-  if ((err = launch(0))) return err;
-  for (unsigned long ci = 1; ci < nchunks; ++ci) {
-    if (ci >= 2 && (err = scatter(ci - 2))) return err;  // frees slot ci&1
+  unsigned long ci = 0;
+  for (; ci < nchunks; ++ci) {
+    if (ci >= 2 && (err = drain(ci - 1))) return err;  // chunk ci-2: frees slot ci&1
+    if (!outputs_uniform(ci)) break;
     gather(ci);
-    if (nonfin[ci]) {
+    if (mixed[ci]) break;
+    if (nonfin[ci]) {  // chunk 0: before any output is written
       cudaStreamSynchronize(p->cv[0].st);
       cudaStreamSynchronize(p->cv[1].st);
       return set_err(MPFFT_ENONFINITE, "input holds NaN or infinity");
     }
     if ((err = launch(ci))) return err;
   }
-  for (unsigned long ci = nchunks >= 2 ? nchunks - 2 : 0; ci < nchunks; ++ci)
-    if ((err = scatter(ci))) return err;
+  if ((err = drain(ci))) return err;
+  *done = std::min(batch, ci * chunk);
   return set_err(MPFFT_OK, "");
 }
 
@@ -996,14 +1017,36 @@ static int mp_tc_check(const mpfft_mp_plan *p, int rc) {
   return rc;
 }
 
+static int mp_execute_hostconv(mpfft_mp_plan *p, unsigned long batch, int mode, const IoShape &ii, mpfr_t *inr,
+                               mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj);
+
 static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, int mode, const IoShape &ii, mpfr_t *inr,
                            mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj) {
   if (p->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
   std::lock_guard<std::mutex> g(p->mu);
   if (!p->force_host_conversion) {
-    const int r = mp_execute_gpuconv(p, batch, mode, ii, inr, ini, oo, outr, outi, fadj);
-    if (r != -1) return mp_tc_check(p, r);
+    unsigned long done = 0;
+    const int r = mp_execute_gpuconv(p, batch, mode, ii, inr, ini, oo, outr, outi, fadj, &done);
+    if (r != MPFFT_OK || done == batch) return mp_tc_check(p, r);
+    if (done > 0) {  // signals [done, batch): the same arrays seen from signal `done` on
+      IoShape ri = ii, ro = oo;
+      for (int c = 0; c < 2; ++c) {
+        if (ri.base[c]) ri.base[c] += done;
+        if (ro.base[c]) ro.base[c] += done;
+      }
+      mpfr_t *r_inr = ii.base[0] ? inr : inr + done * ii.pitch, *r_ini = ii.base[1] ? ini : ini + done * ii.pitch;
+      mpfr_t *r_outr = oo.base[0] ? outr : outr + done * oo.pitch;
+      mpfr_t *r_outi = oo.base[1] ? outi : outi + done * oo.pitch;
+      return mp_execute_hostconv(p, batch - done, mode, ri, r_inr, r_ini, ro, r_outr, r_outi, fadj);
+    }
   }
+  return mp_execute_hostconv(p, batch, mode, ii, inr, ini, oo, outr, outi, fadj);
+}
+
+// Host conversion (mpfr_t <-> limb planes on the CPU) of a whole batch; any mix
+// of precisions.  The caller holds the plan's lock.
+static int mp_execute_hostconv(mpfft_mp_plan *p, unsigned long batch, int mode, const IoShape &ii, mpfr_t *inr,
+                               mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj) {
   if ((unsigned long long)batch * p->pts_max() > (unsigned long long)INT32_MAX)
     return set_err(MPFFT_EUNSUPPORTED, "batch too large for host conversion");
   if (int e = mp_reserve(p, batch)) return e;

@@ -229,6 +229,36 @@ def test_mp_gpu_conversion_matches_host_conversion(M, orc, n, p_in, p_out, batch
     assert L.orc_mp_count_diff(yi.ptr, zi.ptr, n * batch) == 0
 
 
+@pytest.mark.parametrize("what,sig", [("input", 5), ("input", 300), ("output", 520), ("output", 0)])
+def test_mp_precision_change_mid_batch(M, orc, what, sig):
+    """A batch whose precisions change part way (input limb count or output
+    precision of one signal): the GPU-conversion pipeline (chunks of 256
+    signals here) completes the chunks before the change and the remaining
+    signals are converted on the host; every output is bit-identical to a
+    host-conversion plan's."""
+    O = orc
+    L = O.lib()
+    n, p, batch = 16, 128, 600
+    xr, xi = O.mp_pair(n * batch, p)
+    O.fill_uniform(xr, xi, 91)
+    yr, yi = O.mp_pair(n * batch, p)
+    zr, zi = O.mp_pair(n * batch, p)
+    off = sig * n * 32
+    if what == "input":
+        for a in (xr, xi):
+            L.orc_mp_set_prec_all(a.ptr + off, n, 300)
+        L.orc_mp_fill_uniform(xr.ptr + off, xi.ptr + off, n, 7)
+    else:
+        for a in (yr, yi, zr, zi):
+            L.orc_mp_set_prec_all(a.ptr + off, n, 100)
+    gpu = M.MpPlan(n, p)
+    host = M.MpPlan(n, p, host_conversion=True)
+    gpu.execute(batch, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
+    host.execute(batch, xr.ptr, xi.ptr, zr.ptr, zi.ptr)
+    assert L.orc_mp_count_diff(yr.ptr, zr.ptr, n * batch) == 0
+    assert L.orc_mp_count_diff(yi.ptr, zi.ptr, n * batch) == 0
+
+
 @pytest.mark.parametrize("n,p", [(256, 256), (1024, 1024), (4, 64)])
 def test_mp_inverse_entry(M, orc, n, p):
     """mp_sr24_cp_ifft = the reference's test() inverse (swap, forward, swap,
