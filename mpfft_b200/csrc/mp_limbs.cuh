@@ -85,9 +85,19 @@ __device__ __forceinline__ void combine_p(uint32_t (&x)[L], const uint32_t *p, s
 // is a 32x32+32+32 -> 64-bit multiply-add (it cannot overflow), written in
 // plain C so the compiler can schedule the two halves freely; on sm_100a this
 // issues faster than PTX mad.lo.cc/madc.hi.cc chains (measured).
-template <int L>
+//
+// kPacked: w holds the L limbs contiguously in shared memory, 16-byte aligned
+// (tplane unused); they are read four at a time with 128-bit loads.
+template <int L, bool kPacked = false>
 __device__ __forceinline__ void mul_tw(uint32_t (&x)[L], const uint32_t *w, size_t tplane) {
   static_assert(L >= 2, "fixed-point product needs at least two limbs");
+  // limb j of the twiddle: p points at it (strided planes) or at limb 0 (packed)
+  uint4 v4;  // packed: limbs 4*(j/4) .. 4*(j/4)+3
+  auto limb = [&](const uint32_t *p, int j) -> uint32_t {
+    if (!kPacked) return *p;
+    if ((j & 3) == 0) v4 = *reinterpret_cast<const uint4 *>(p + j);
+    return (j & 3) == 0 ? v4.x : (j & 3) == 1 ? v4.y : (j & 3) == 2 ? v4.z : v4.w;
+  };
   const uint32_t smask = 0u - (x[L - 1] >> 31);
 
   // acc[a] holds column (L-2+a), a = 0 .. L+1
@@ -98,8 +108,8 @@ __device__ __forceinline__ void mul_tw(uint32_t (&x)[L], const uint32_t *w, size
 
   const uint32_t *w0 = w;
 #pragma unroll
-  for (int j = 0; j < L; ++j, w += tplane) {
-    const uint32_t t = *w;
+  for (int j = 0; j < L; ++j, w += kPacked ? 0 : tplane) {
+    const uint32_t t = limb(w, j);
     const int i0 = (L - 2 - j) > 0 ? (L - 2 - j) : 0;
     uint32_t c = 0;
 #pragma unroll
@@ -114,7 +124,7 @@ __device__ __forceinline__ void mul_tw(uint32_t (&x)[L], const uint32_t *w, size
   {
     uint32_t c = 1;
 #pragma unroll
-    for (int j = 0; j < L; ++j, w0 += tplane) acc[j + 2] = addc(acc[j + 2], ~(*w0 & smask), c);
+    for (int j = 0; j < L; ++j, w0 += kPacked ? 0 : tplane) acc[j + 2] = addc(acc[j + 2], ~(limb(w0, j) & smask), c);
   }
   // x = (columns L-1 .. 2L-1) >> 31
 #pragma unroll

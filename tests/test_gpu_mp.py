@@ -89,10 +89,13 @@ def test_mp_v2_and_scaled(M, orc):
     assert L.orc_mp_count_diff(yr.ptr, sr.ptr, n) == 0 and L.orc_mp_count_diff(yi.ptr, si.ptr, n) == 0
 
 
-@pytest.mark.parametrize("n,p,batch", [(128, 256, 5), (128, 1024, 32), (64, 100, 64)])
+@pytest.mark.parametrize("n,p,batch", [(128, 256, 5), (128, 1024, 32), (64, 100, 64), (16, 64, 256), (64, 512, 128),
+                                       (32, 960, 128)])
 def test_mp_batch_equals_single_calls(M, orc, n, p, batch):
-    """Batches that are a multiple of 32 run the warp-per-butterfly kernel,
-    others and single signals the thread-per-butterfly kernel: all bit-equal."""
+    """Batched and single-signal calls are bit-equal.  In a batch that is a
+    multiple of 32 every warp shares one butterfly index; in a multiple of 128
+    (3, 17 and 31 limbs here) every CTA does, and the level kernel stages its
+    twiddles in shared memory; single signals read them from global memory."""
     O = orc
     xr, xi = O.mp_pair(n * batch, p)
     O.fill_uniform(xr, xi, 31)
