@@ -166,9 +166,9 @@ constexpr int level_min_blocks() {
 // Batches that are a multiple of the CTA size give every CTA one (node, k):
 // up to 31 limbs the CTA then stages its three twiddles in shared memory once
 // and the products read them four limbs per load (measured at N=1024, batch
-// 2048: +4.6 % at 9 limbs, +3.1 % at 17, +2.2 % at 31; -0.7 % at 33, where the
-// 128-register product already spills, so the larger limb counts keep the
-// per-row global loads).
+// 2048: +4.6 % at 9 limbs, +3.1 % at 17, +0.4 to +2.2 % at 31; -0.7 % at 33,
+// where the 128-register product already spills, so the larger limb counts
+// keep the per-row global loads).
 constexpr int kPackedTwiddleMaxLimbs = 31;
 
 template <int L, bool kPackedTw>
