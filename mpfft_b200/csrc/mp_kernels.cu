@@ -274,8 +274,137 @@ __global__ void __launch_bounds__(128, level_min_blocks<L>()) mp_level_kernel(ui
 }
 
 // ---------------------------------------------------------------------------
+// the same launch for batches too small to fill the GPU
+// ---------------------------------------------------------------------------
+//
+// mp_level_kernel runs a butterfly's six products one after another on one
+// thread, so with few butterflies (one signal: n/4 per launch) each launch
+// takes six product latencies.  Here the six steps of a butterfly run on six
+// threads at once: every thread forms its step's product into shared memory;
+// after a barrier the threads of steps 1 and 2 merge theirs with the side's
+// first product and store it into the Z slot exactly as mp_level_kernel does;
+// after a second barrier one thread runs the L-combine.  Same operations on
+// the same operands, so the results are bit-identical.
+
+// Step st (0..5) of a twiddled butterfly: side st/3 (0: Z+ at zp, 1: Z- at
+// zm), step st%3.  X = pa (+ or - pb when pb is set), X *= the twiddle whose
+// first limb w points at (cos, cos+sin or |cos-sin|) when mul, else X = 0;
+// then either X becomes the side's first product P (dst null) or
+// dst = (negx ? -X : X) + sp * P.  This is the step table of mp_level_kernel,
+// which spells it out inline in its step loop (the struct form measured 4 %
+// slower there); the two kernels are checked to be bit-identical.
+struct BflyStep {
+  const uint32_t *pa, *pb, *w;  // w: the twiddle row's first limb (planes)
+  uint32_t *dst;
+  int sp;
+  bool sub, negx, mul;
+};
+
+__device__ __forceinline__ BflyStep bfly_step(int st_, bool special, bool dn, uint32_t *zp, uint32_t *zm,
+                                              size_t cim, const uint32_t *wr, const uint32_t *ws,
+                                              const uint32_t *wd) {
+  const int side = st_ >= 3;
+  const int step = st_ - 3 * side;
+  uint32_t *zr = side ? zm : zp;
+  uint32_t *zi = zr + cim;
+  BflyStep S{zr, nullptr, wr, nullptr, 0, false, false, true};
+  if (step == 0) {
+    S.pb = zi;
+    S.sub = side;
+  } else if (!special) {
+    if (step == 1) {
+      S.pa = zi;
+      S.w = wd;
+      S.negx = dn ^ (side == 0);
+      S.sp = 1;
+      S.dst = zi;
+    } else {
+      S.w = ws;
+      S.negx = (side == 0);
+      S.sp = side ? -1 : 1;
+      S.dst = zr;
+    }
+  } else {
+    if (step == 1) {
+      S.pa = side ? zr : zi;
+      S.pb = side ? zi : zr;
+      S.sub = !side;
+      S.dst = zr;
+    } else {
+      S.mul = false;
+      S.sp = 1;
+      S.dst = zi;
+    }
+  }
+  return S;
+}
+
+constexpr int kSmallBflies = 16;  // butterflies per CTA (96 threads)
+
+template <int L>
+__global__ void __launch_bounds__(6 * kSmallBflies) mp_level_small_kernel(uint32_t *__restrict__ y, int N, int B,
+                                                                          int n, const int *__restrict__ node_off,
+                                                                          int nnodes, const uint32_t *__restrict__ tw,
+                                                                          const uint8_t *__restrict__ dneg, int tws) {
+  __shared__ uint32_t Qs[kSmallBflies * 6 * L];  // [butterfly][step][limb]
+  const int lb = threadIdx.x / 6, st_ = threadIdx.x - 6 * lb;
+  const int q = n >> 2;
+  const long long t = (long long)blockIdx.x * kSmallBflies + lb;
+  const bool valid = t < (long long)nnodes * q * B;
+  int k = 0;
+  uint32_t *u0 = nullptr, *u1 = nullptr, *zp = nullptr, *zm = nullptr;
+  const size_t plane = (size_t)N * B;
+  const size_t cim = (size_t)L * plane;
+  BflyStep S{};
+  uint32_t *Q = Qs + (size_t)(lb * 6 + st_) * L;
+  if (valid) {
+    const int b = (int)(t % B);
+    const long long r = t / B;
+    k = (int)(r % q);
+    const int off = node_off[r / q];
+    u0 = y + (size_t)(off + k) * B + b;
+    u1 = u0 + (size_t)q * B;
+    zp = u0 + (size_t)2 * q * B;
+    zm = u0 + (size_t)3 * q * B;
+    if (k != 0) {
+      const size_t tplane = (size_t)(N >> 2) * tws;
+      const int kn = k * (N / n) * tws;
+      const bool special = (2 * k == q);
+      const bool dn = special ? false : (dneg[kn] != 0);
+      S = bfly_step(st_, special, dn, zp, zm, cim, tw + kn, tw + (size_t)L * tplane + kn,
+                    tw + (size_t)2 * L * tplane + kn);
+      uint32_t X[L];
+      if (S.mul) {
+        ld_addsub<L>(X, S.pa, S.pb, plane, S.sub);
+        mul_tw<L>(X, S.w, tplane);
+      } else {
+#pragma unroll
+        for (int i = 0; i < L; ++i) X[i] = 0;
+      }
+      st<L>(Q, 1, X);
+    }
+  }
+  __syncthreads();
+  if (valid && k != 0 && S.dst) {  // steps 1 and 2: merge with the side's first product
+    uint32_t X[L];
+    ld<L>(X, Q, 1);
+    combine_p<L>(X, Qs + (size_t)(lb * 6 + (st_ >= 3 ? 3 : 0)) * L, 1, S.negx, S.sp);
+    st<L>(S.dst, plane, X);
+  }
+  __syncthreads();  // the merged Z slots (global) are visible to the CTA
+  if (valid && st_ == 0) combine<L>(u0, u1, zp, zm, plane, cim, k != 0);
+}
+
+// ---------------------------------------------------------------------------
 // host-side launchers, one instantiation per supported limb count
 // ---------------------------------------------------------------------------
+
+// Below this many butterflies mp_level_kernel would occupy at most a quarter
+// of the SMs with one CTA each, and the level runs as mp_level_small_kernel
+// (measured at N=1024, P=1024: one signal 2.0k -> 5.2k transforms/s; with
+// 256 signals, 65k butterflies per launch, the one-thread-per-butterfly
+// kernel is 1.5x faster).
+constexpr long long kSmallLevelButterflies = 148LL * 32;
 
 template <int L>
 static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
@@ -295,7 +424,10 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
     const int lthreads = 128;
     const int blocks = (int)((total + lthreads - 1) / lthreads);
     timer.begin();
-    if (L <= kPackedTwiddleMaxLimbs && B % lthreads == 0)
+    if (total < kSmallLevelButterflies)
+      mp_level_small_kernel<L><<<(unsigned)((total + kSmallBflies - 1) / kSmallBflies), 6 * kSmallBflies, 0, s>>>(
+          out, T.N, B, n, T.node_off + T.level_start[lv], T.level_count[lv], T.tw, T.dneg, T.tws);
+    else if (L <= kPackedTwiddleMaxLimbs && B % lthreads == 0)
       mp_level_kernel<L, (L <= kPackedTwiddleMaxLimbs)><<<blocks, lthreads, 0, s>>>(
           out, T.N, B, n, T.node_off + T.level_start[lv], T.level_count[lv], T.tw, T.dneg, T.tws);
     else

@@ -115,6 +115,37 @@ def test_mp_batch_equals_single_calls(M, orc, n, p, batch):
         assert L.orc_mp_count_diff(si.ptr, yi.ptr + b * n * 32, n) == 0
 
 
+@pytest.mark.parametrize("p", [1024, 512, 100])
+def test_mp_small_batch_level_kernel_bit_identical(M, p):
+    """Level launches with fewer butterflies than one wave of the main level
+    kernel run one thread per product (mp_level_small_kernel).  On the same
+    limb planes, a batch of 2048 signals at N=1024 (every level on the main
+    kernel) and single signals cut from it (every level on the small kernel)
+    give bit-identical outputs."""
+    import torch
+
+    from mpfft_b200.profile_case import synthetic_planes
+
+    n, B = 1024, 2048
+    plan = M.MpPlan(n, p)
+    Lm = plan.limbs
+    host = synthetic_planes(n, Lm, plan.frac_bits, B, seed=3)
+    s = torch.cuda.current_stream().cuda_stream
+    d_in = torch.from_numpy(host.view(np.int32)).cuda()
+    d_out = torch.empty_like(d_in)
+    plan.execute_device(B, d_in.data_ptr(), d_out.data_ptr(), s)
+    torch.cuda.synchronize()
+    big = d_out.cpu().numpy().view(np.uint32).reshape(2, Lm, n, B)
+    planes = host.reshape(2, Lm, n, B)
+    for b in (0, 1, 1000, B - 1):
+        one = np.ascontiguousarray(planes[:, :, :, b]).reshape(-1)
+        d1 = torch.from_numpy(one.view(np.int32)).cuda()
+        o1 = torch.empty_like(d1)
+        plan.execute_device(1, d1.data_ptr(), o1.data_ptr(), s)
+        torch.cuda.synchronize()
+        assert np.array_equal(o1.cpu().numpy().view(np.uint32).reshape(2, Lm, n), big[:, :, :, b]), b
+
+
 def test_mp_device_api_matches_host_api(M, orc):
     import torch
 
