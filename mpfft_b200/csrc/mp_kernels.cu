@@ -399,12 +399,14 @@ __global__ void __launch_bounds__(6 * kSmallBflies) mp_level_small_kernel(uint32
 // host-side launchers, one instantiation per supported limb count
 // ---------------------------------------------------------------------------
 
-// Below this many butterflies mp_level_kernel would occupy at most a quarter
-// of the SMs with one CTA each, and the level runs as mp_level_small_kernel
-// (measured at N=1024, P=1024: one signal 2.0k -> 5.2k transforms/s; with
-// 256 signals, 65k butterflies per launch, the one-thread-per-butterfly
-// kernel is 1.5x faster).
-constexpr long long kSmallLevelButterflies = 148LL * 32;
+// Below this many butterflies mp_level_kernel would run at most one CTA per
+// SM, and the level runs as mp_level_small_kernel.  Measured at N=1024,
+// P=1024 (transforms/s): one signal 2.0k -> 5.2k; 32 signals 95k -> 126k
+// (with 148 x 32 as the threshold instead of 148 x 128: 95k); 64 signals
+// 180k -> 200k; at 128 signals within 3 % either way; 148 x 256 as the
+// threshold loses 17 % at 128 signals, and with 256 signals (65k butterflies
+// per launch) the one-thread-per-butterfly kernel is 1.5x faster.
+constexpr long long kSmallLevelButterflies = 148LL * 128;
 
 template <int L>
 static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
