@@ -99,6 +99,80 @@ __global__ void __launch_bounds__(256) mp_leaf_kernel(const uint32_t *__restrict
   }
 }
 
+// The same leaves for launches too small to fill the GPU: one thread per
+// output component (8 for a 4-point leaf, 4 for a 2-point one, 2 for a copy),
+// each loading its (at most four) input components for every limb at once and
+// then running that output's carry chain -- the chains of mp_leaf_kernel are
+// already one per output, so the results are bit-identical.  16 leaves per CTA.
+template <int L>
+__global__ void __launch_bounds__(128) mp_leaf_small_kernel(const uint32_t *__restrict__ in,
+                                                            uint32_t *__restrict__ out, int N, int B,
+                                                            const MpLeaf *__restrict__ leaves, int nleaves) {
+  const long long t = (long long)blockIdx.x * 16 + (threadIdx.x >> 3);
+  const int o = threadIdx.x & 7;
+  if (t >= (long long)nleaves * B) return;
+  const int b = (int)(t % B);
+  const MpLeaf lf = leaves[t / B];
+  if (o >= 2 * lf.n) return;
+  const size_t plane = (size_t)N * B;
+  const size_t cim = (size_t)L * plane;
+  // terms of output o: (input element j, imaginary part?, sign)
+  int nt = 0, tj[4] = {0, 0, 0, 0}, ti[4] = {0, 0, 0, 0}, ts[4] = {1, 1, 1, 1};
+  if (lf.n == 4) {
+    // X0 = x0+x2 + (x1+x3)      X2 = x0+x2 - (x1+x3)
+    // X1 = x0-x2 - i(x1-x3)     X3 = x0-x2 + i(x1-x3)
+    const int im = o >= 4, q = o & 3;
+    nt = 4;
+    tj[0] = 0, ti[0] = im;
+    tj[1] = 2, ti[1] = im, ts[1] = (q & 1) ? -1 : 1;
+    tj[2] = 1, tj[3] = 3;
+    if ((q & 1) == 0) {  // X0, X2: the same part of x1, x3
+      ti[2] = ti[3] = im;
+      ts[2] = ts[3] = q == 0 ? 1 : -1;
+    } else {  // X1, X3: the other part of x1, x3
+      ti[2] = ti[3] = !im;
+      const int sg = ((q == 1) != (im != 0)) ? 1 : -1;  // X1r: +(x1i-x3i), X1i: -(x1r-x3r), X3 opposite
+      ts[2] = sg, ts[3] = -sg;
+    }
+  } else if (lf.n == 2) {
+    nt = 2;
+    tj[1] = 1, ti[0] = ti[1] = o >= 2, ts[1] = (o & 1) ? -1 : 1;
+  } else {
+    nt = 1;
+    ti[0] = o;
+  }
+  const uint32_t *src[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int j = e < nt ? tj[e] : 0;
+    const int idx = (j == 0 && lf.sn < 0) ? lf.sn + N : lf.sn + j * lf.s;
+    src[e] = in + (size_t)idx * B + b + (ti[e] ? cim : 0);
+  }
+  const int q = lf.n == 4 ? (o & 3) : (lf.n == 2 ? (o & 1) : 0);
+  const bool im_out = lf.n == 4 ? o >= 4 : (lf.n == 2 ? o >= 2 : o == 1);
+  uint32_t *y = out + ((size_t)lf.out + q) * B + b + (im_out ? cim : 0);
+  uint32_t v[4][L];
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+    if (e < nt) {
+#pragma unroll
+      for (int i = 0; i < L; ++i) v[e][i] = src[e][(size_t)i * plane];
+    }
+  int64_t c = 0;
+#pragma unroll
+  for (int i = 0; i < L; ++i) {
+    int64_t acc = c;
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (e < nt) {
+        const int64_t x = (i == L - 1) ? (int64_t)(int32_t)v[e][i] : (int64_t)v[e][i];
+        acc += ts[e] > 0 ? x : -x;
+      }
+    y[(size_t)i * plane] = (uint32_t)acc;
+    c = acc >> 32;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // L-shaped combine of one butterfly (reference :238-252), streamed limb by
 // limb: a1 = m1 + m2, a2 = m1 - m2, then U0 +/- a1 and U1 -/+ i a2, twelve
@@ -456,9 +530,12 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
   LaunchTimer timer(launch_ms, s);
   {
     const long long total = (long long)T.nleaves * B;
-    const int blocks = (int)((total + threads - 1) / threads);
     timer.begin();
-    mp_leaf_kernel<L><<<blocks, threads, 0, s>>>(in, out, T.N, B, T.leaves, T.nleaves);
+    if (total < kSmallLevelButterflies)
+      mp_leaf_small_kernel<L><<<(unsigned)((total + 15) / 16), 128, 0, s>>>(in, out, T.N, B, T.leaves, T.nleaves);
+    else
+      mp_leaf_kernel<L><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(in, out, T.N, B, T.leaves,
+                                                                                    T.nleaves);
     timer.end();
   }
   for (int lv = 0; lv < T.nlevels; ++lv) {
