@@ -52,6 +52,9 @@ def parse_args():
     ap.add_argument("--batch", type=int, default=2048, help="signals per GPU per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--dropin", action="store_true",
+                    help="instead of the contract line: latency of one mp_sr24_cp_fft call (one signal of --n points "
+                         "at --prec bits, host mpfr_t arrays) next to the reference's serial and OpenMP-4 code")
     return ap.parse_args()
 
 
@@ -201,6 +204,44 @@ def level_mults(n: int) -> int:
     return 4 + 6 * (q - 2)
 
 
+def dropin_arm(args):
+    """One signal per call through the drop-in mp_sr24_cp_fft (the way the
+    reference's own driver calls its transform, mpFFT.c:47): host mpfr_t arrays
+    in and out, conversion, copies, kernels and synchronisation inside each
+    call; wall time per call over many calls.  Beside it the reference's serial
+    code (lab/serial/mp/serial_mp_fft3.c) and its OpenMP code
+    (lab/parallel/mp/parallel_mp_fft2.c, 4 threads) on the same N and P."""
+    import mpfft_b200 as M
+    from mpfft_b200 import mparray
+    from oracle import oracle as O
+
+    n, p = args.n, args.prec
+    xr, xi = mparray.MpfrArray(n, p), mparray.MpfrArray(n, p)
+    mparray.fill_uniform(xr, xi, SEED)
+    yr, yi = mparray.MpfrArray(n, p), mparray.MpfrArray(n, p)
+    for _ in range(20):
+        if M.mp_sr24_cp_fft(n, 1, 0, xr.ptr, xi.ptr, yr.ptr, yi.ptr) != M.OK:
+            raise RuntimeError(M.last_error())
+    reps = 300
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        M.mp_sr24_cp_fft(n, 1, 0, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
+    us = (time.perf_counter() - t0) / reps * 1e6
+    ser = omp = None
+    if O.ref_available("mp_ser"):
+        t1 = _ref_worker("mp_ser", n, p, 3, SEED) / 3
+        m = max(3, int(2e9 / t1))
+        ser = _ref_worker("mp_ser", n, p, m, SEED) / m / 1e3
+    if O.ref_available("mp_par"):
+        m = max(3, int(1e9 / (ser * 1e3))) if ser else 3
+        omp = _ref_worker("mp_par", n, p, m, SEED) / m / 1e3
+    print(json.dumps({"metric": "drop-in call latency: one signal per mp_sr24_cp_fft call, host mpfr_t arrays",
+                      "value": us, "unit": "us", "higher_is_better": False, "calls_per_s": 1e6 / us,
+                      "config": {"n": n, "prec_bits": p, "calls": reps},
+                      "reference_serial_us": ser, "reference_omp4_us": omp,
+                      "speedup_vs_serial": (ser / us) if ser else None}))
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -209,6 +250,10 @@ def main():
 
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.dropin:
+        if rank == 0:
+            dropin_arm(args)
         return
 
     # CPU baseline before any CUDA work (spawned worker processes)
