@@ -438,9 +438,10 @@ struct mpfft_mp_plan {
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
     uint32_t *d_in = nullptr, *d_out = nullptr;
-    uint64_t *h_mi = nullptr, *d_mi = nullptr, *h_mo = nullptr, *d_mo = nullptr;
-    int64_t *h_ei = nullptr, *d_ei = nullptr, *h_eo = nullptr, *d_eo = nullptr, *d_es = nullptr;
-    uint8_t *h_si = nullptr, *d_si = nullptr, *h_so = nullptr, *d_so = nullptr;
+    // raw MPFR fields in (i) and out (o), pinned host and device: one block
+    // per direction laid out per chunk by stage_view (one copy each way)
+    uint64_t *h_i = nullptr, *d_i = nullptr, *h_o = nullptr, *d_o = nullptr;
+    int64_t *d_es = nullptr;
     uint32_t *d_big = nullptr;  // streaming-kernel scratch of this slot (L > kMaxLimbs)
     uint32_t *d_tmp = nullptr;  // transposition buffer of this slot (multi-dimensional plans)
   };
@@ -449,11 +450,10 @@ struct mpfft_mp_plan {
   int cv_nli = 0, cv_nlo = 0;
   void free_conv() {
     for (auto &c : cv) {
-      for (void *q : {(void *)c.d_in, (void *)c.d_out, (void *)c.d_mi, (void *)c.d_mo, (void *)c.d_ei,
-                      (void *)c.d_eo, (void *)c.d_es, (void *)c.d_si, (void *)c.d_so, (void *)c.d_big,
-                      (void *)c.d_tmp})
+      for (void *q : {(void *)c.d_in, (void *)c.d_out, (void *)c.d_i, (void *)c.d_o, (void *)c.d_es,
+                      (void *)c.d_big, (void *)c.d_tmp})
         if (q) cudaFree(q);
-      for (void *q : {(void *)c.h_mi, (void *)c.h_mo, (void *)c.h_ei, (void *)c.h_eo, (void *)c.h_si, (void *)c.h_so})
+      for (void *q : {(void *)c.h_i, (void *)c.h_o})
         if (q) cudaFreeHost(q);
       if (c.st) cudaStreamDestroy(c.st);
       if (c.done) cudaEventDestroy(c.done);
@@ -739,6 +739,22 @@ static cudaError_t mp_transform(const mpfft_mp_plan *p, const uint32_t *in, uint
   return cudaSuccess;
 }
 
+// Raw MPFR fields of n components with nl significand limbs each, packed in
+// one buffer: limbs [n][nl], then exponents [n], then sign bytes [n].  The
+// same view of a pinned host block and of a device block makes each
+// direction of a chunk one copy of `bytes`.
+struct StageView {
+  uint64_t *m;
+  int64_t *e;
+  uint8_t *s;
+  size_t bytes;
+};
+static inline size_t stage_bytes(size_t n, int nl) { return n * ((size_t)nl * 8 + 8 + 1); }
+static inline StageView stage_view(uint64_t *base, size_t n, int nl) {
+  int64_t *e = reinterpret_cast<int64_t *>(base + n * (size_t)nl);
+  return StageView{base, e, reinterpret_cast<uint8_t *>(e + n), stage_bytes(n, nl)};
+}
+
 static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int nlo) {
   if (chunk <= p->cv_chunk && nli <= p->cv_nli && nlo <= p->cv_nlo) return MPFFT_OK;
   p->free_conv();
@@ -752,18 +768,10 @@ static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int n
     ok = ok && cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) == cudaSuccess;
     dm((void **)&c.d_in, words * 4);
     dm((void **)&c.d_out, words * 4);
-    dm((void **)&c.d_mi, comp * nli * 8);
-    hm((void **)&c.h_mi, comp * nli * 8);
-    dm((void **)&c.d_mo, comp * nlo * 8);
-    hm((void **)&c.h_mo, comp * nlo * 8);
-    dm((void **)&c.d_ei, comp * 8);
-    hm((void **)&c.h_ei, comp * 8);
-    dm((void **)&c.d_eo, comp * 8);
-    hm((void **)&c.h_eo, comp * 8);
-    dm((void **)&c.d_si, comp);
-    hm((void **)&c.h_si, comp);
-    dm((void **)&c.d_so, comp);
-    hm((void **)&c.h_so, comp);
+    dm((void **)&c.d_i, stage_bytes(comp, nli));
+    hm((void **)&c.h_i, stage_bytes(comp, nli));
+    dm((void **)&c.d_o, stage_bytes(comp, nlo));
+    hm((void **)&c.h_o, stage_bytes(comp, nlo));
     dm((void **)&c.d_es, chunk * 8);
     if (const size_t bw = mp_plan_big_words(p, chunk)) dm((void **)&c.d_big, bw * 4);
     if (p->rank > 1) dm((void **)&c.d_tmp, words * 4);
@@ -854,6 +862,7 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
   auto gather = [&](unsigned long ci) {
     auto &c = p->cv[ci & 1];
     const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
+    const StageView hv = stage_view(c.h_i, (size_t)2 * Ni * cb, nli);
     parallel_for((long)(2 * cb * Ni), 2048, [&](long x0, long x1) {
       constexpr long kAhead = 8;  // significands prefetched ahead of use
       auto at = [&](long u) {
@@ -874,13 +883,13 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
         }
         if (x->_mpfr_exp <= LONG_MIN + 3) {  // MPFR's reserved exponents: zero, NaN, infinity
           if (!mpfr_zero_p(x)) nonfin[ci] = 1;
-          stage_word(c.h_ei + u, INT64_MIN);
-          c.h_si[u] = 0;
-          memset(c.h_mi + u * nli, 0, nli * 8);
+          stage_word(hv.e + u, INT64_MIN);
+          hv.s[u] = 0;
+          memset(hv.m + u * nli, 0, nli * 8);
         } else {
-          stage_word(c.h_ei + u, x->_mpfr_exp);
-          c.h_si[u] = x->_mpfr_sign < 0;
-          stage_limbs(c.h_mi + u * nli, reinterpret_cast<const uint64_t *>(x->_mpfr_d), nli);
+          stage_word(hv.e + u, x->_mpfr_exp);
+          hv.s[u] = x->_mpfr_sign < 0;
+          stage_limbs(hv.m + u * nli, reinterpret_cast<const uint64_t *>(x->_mpfr_d), nli);
         }
       }
       stage_fence();
@@ -890,18 +899,15 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
     auto &c = p->cv[ci & 1];
     const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
     const size_t ci_n = (size_t)2 * Ni * cb, co_n = (size_t)2 * No * cb;
-    CUDA_TRY(cudaMemcpyAsync(c.d_mi, c.h_mi, ci_n * nli * 8, cudaMemcpyHostToDevice, c.st));
-    CUDA_TRY(cudaMemcpyAsync(c.d_ei, c.h_ei, ci_n * 8, cudaMemcpyHostToDevice, c.st));
-    CUDA_TRY(cudaMemcpyAsync(c.d_si, c.h_si, ci_n, cudaMemcpyHostToDevice, c.st));
-    CUDA_TRY(mp_import_launch(c.d_mi, c.d_ei, c.d_si, nli, (int)Ni, (int)cb, p->L, p->F, c.d_es, c.d_in, c.st,
+    const StageView di = stage_view(c.d_i, ci_n, nli), dout = stage_view(c.d_o, co_n, nlo);
+    CUDA_TRY(cudaMemcpyAsync(c.d_i, c.h_i, di.bytes, cudaMemcpyHostToDevice, c.st));
+    CUDA_TRY(mp_import_launch(di.m, di.e, di.s, nli, (int)Ni, (int)cb, p->L, p->F, c.d_es, c.d_in, c.st,
                               true));
     uint32_t *res = nullptr;
     CUDA_TRY(mp_device_pipeline(p, mode, c.d_in, c.d_out, (int)cb, c.st, c.d_big, c.d_tmp, &res));
-    CUDA_TRY(mp_export_launch(res, (int)No, (int)cb, p->L, c.d_es, p->F + fadj, prec_out, nlo, c.d_mo, c.d_eo,
-                              c.d_so, c.st, true));
-    CUDA_TRY(cudaMemcpyAsync(c.h_mo, c.d_mo, co_n * nlo * 8, cudaMemcpyDeviceToHost, c.st));
-    CUDA_TRY(cudaMemcpyAsync(c.h_eo, c.d_eo, co_n * 8, cudaMemcpyDeviceToHost, c.st));
-    CUDA_TRY(cudaMemcpyAsync(c.h_so, c.d_so, co_n, cudaMemcpyDeviceToHost, c.st));
+    CUDA_TRY(mp_export_launch(res, (int)No, (int)cb, p->L, c.d_es, p->F + fadj, prec_out, nlo, dout.m, dout.e,
+                              dout.s, c.st, true));
+    CUDA_TRY(cudaMemcpyAsync(c.h_o, c.d_o, dout.bytes, cudaMemcpyDeviceToHost, c.st));
     CUDA_TRY(cudaEventRecord(c.done, c.st));
     return MPFFT_OK;
   };
@@ -909,6 +915,7 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
     auto &c = p->cv[ci & 1];
     CUDA_TRY(cudaEventSynchronize(c.done));
     const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
+    const StageView ho = stage_view(c.h_o, (size_t)2 * No * cb, nlo);
     parallel_for((long)(2 * cb * No), 2048, [&](long x0, long x1) {
       constexpr long kAhead = 8;  // destination significands prefetched ahead of use
       auto at = [&](long u) {
@@ -924,18 +931,18 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
         }
         mpfr_ptr y = at(u);
         const size_t t = (size_t)u;  // signal-major staging
-        const int64_t e = c.h_eo[t];
+        const int64_t e = ho.e[t];
         if (e == INT64_MIN) {
           mpfr_set_zero(y, 1);
         } else if (e >= emin && e <= emax) {
-          memcpy(y->_mpfr_d, c.h_mo + t * nlo, nlo * 8);
+          memcpy(y->_mpfr_d, ho.m + t * nlo, nlo * 8);
           y->_mpfr_exp = e;
-          y->_mpfr_sign = c.h_so[t] ? -1 : 1;
+          y->_mpfr_sign = ho.s[t] ? -1 : 1;
         } else {  // outside the current exponent range: let MPFR overflow/underflow
           __mpz_struct z;
           z._mp_alloc = nlo;
-          z._mp_size = c.h_so[t] ? -nlo : nlo;
-          z._mp_d = reinterpret_cast<mp_limb_t *>(c.h_mo + t * nlo);
+          z._mp_size = ho.s[t] ? -nlo : nlo;
+          z._mp_d = reinterpret_cast<mp_limb_t *>(ho.m + t * nlo);
           mpfr_set_z_2exp(y, &z, e - 64L * nlo, MPFR_RNDN);
         }
       }
