@@ -442,6 +442,11 @@ struct mpfft_mp_plan {
     // per direction laid out per chunk by stage_view (one copy each way)
     uint64_t *h_i = nullptr, *d_i = nullptr, *h_o = nullptr, *d_o = nullptr;
     int64_t *d_es = nullptr;
+    // the chunk's copies and kernels captured as a CUDA graph, per chunk shape
+    // (null: the shape runs its launches directly); uses[] counts the direct
+    // runs before a shape is captured
+    std::map<std::vector<long>, cudaGraphExec_t> graphs;
+    std::map<std::vector<long>, int> uses;
     uint32_t *d_big = nullptr;  // streaming-kernel scratch of this slot (L > kMaxLimbs)
     uint32_t *d_tmp = nullptr;  // transposition buffer of this slot (multi-dimensional plans)
   };
@@ -450,6 +455,8 @@ struct mpfft_mp_plan {
   int cv_nli = 0, cv_nlo = 0;
   void free_conv() {
     for (auto &c : cv) {
+      for (auto &g : c.graphs)
+        if (g.second) cudaGraphExecDestroy(g.second);
       for (void *q : {(void *)c.d_in, (void *)c.d_out, (void *)c.d_i, (void *)c.d_o, (void *)c.d_es,
                       (void *)c.d_big, (void *)c.d_tmp})
         if (q) cudaFree(q);
@@ -755,6 +762,8 @@ static inline StageView stage_view(uint64_t *base, size_t n, int nl) {
   return StageView{base, e, reinterpret_cast<uint8_t *>(e + n), stage_bytes(n, nl)};
 }
 
+using ConvSlotRef = mpfft_mp_plan::ConvSlot &;
+
 static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int nlo) {
   if (chunk <= p->cv_chunk && nli <= p->cv_nli && nlo <= p->cv_nlo) return MPFFT_OK;
   p->free_conv();
@@ -895,9 +904,8 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
       stage_fence();
     });
   };
-  auto launch = [&](unsigned long ci) -> int {
-    auto &c = p->cv[ci & 1];
-    const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
+  // copy in, import, transform, export, copy out: one chunk on its slot's stream
+  auto enqueue = [&](ConvSlotRef c, unsigned long cb) -> int {
     const size_t ci_n = (size_t)2 * Ni * cb, co_n = (size_t)2 * No * cb;
     const StageView di = stage_view(c.d_i, ci_n, nli), dout = stage_view(c.d_o, co_n, nlo);
     CUDA_TRY(cudaMemcpyAsync(c.d_i, c.h_i, di.bytes, cudaMemcpyHostToDevice, c.st));
@@ -908,6 +916,39 @@ static int mp_execute_gpuconv(mpfft_mp_plan *p, unsigned long batch, int mode, c
     CUDA_TRY(mp_export_launch(res, (int)No, (int)cb, p->L, c.d_es, p->F + fadj, prec_out, nlo, dout.m, dout.e,
                               dout.s, c.st, true));
     CUDA_TRY(cudaMemcpyAsync(c.h_o, c.d_o, dout.bytes, cudaMemcpyDeviceToHost, c.st));
+    return MPFFT_OK;
+  };
+  // Integer-pipe plans replay a chunk shape from a CUDA graph from its second
+  // use on (one launch instead of a dozen; the first use runs directly so that
+  // nothing is initialised inside a capture).  A capture that fails leaves
+  // the shape on direct launches.
+  const bool graphable = p->L <= kMaxLimbs && !mp_tc_used(p->tabs, p->L);
+  auto launch = [&](unsigned long ci) -> int {
+    auto &c = p->cv[ci & 1];
+    const unsigned long b0 = ci * chunk, cb = std::min(chunk, batch - b0);
+    if (graphable) {
+      const std::vector<long> key{(long)cb, nli, nlo, mode, fadj, prec_out, (long)Ni, (long)No};
+      auto it = c.graphs.find(key);
+      if (it == c.graphs.end() && c.uses[key]++ >= 1) {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        if (cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+          const int e = enqueue(c, cb);
+          const cudaError_t ce = cudaStreamEndCapture(c.st, &g);
+          if (e != MPFFT_OK || ce != cudaSuccess || !g || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+            ge = nullptr;
+          if (g) cudaGraphDestroy(g);
+        }
+        cudaGetLastError();
+        it = c.graphs.emplace(key, ge).first;
+      }
+      if (it != c.graphs.end() && it->second) {
+        CUDA_TRY(cudaGraphLaunch(it->second, c.st));
+        CUDA_TRY(cudaEventRecord(c.done, c.st));
+        return MPFFT_OK;
+      }
+    }
+    if (int e = enqueue(c, cb)) return e;
     CUDA_TRY(cudaEventRecord(c.done, c.st));
     return MPFFT_OK;
   };
