@@ -55,6 +55,8 @@ def parse_args():
     ap.add_argument("--dropin", action="store_true",
                     help="instead of the contract line: latency of one mp_sr24_cp_fft call (one signal of --n points "
                          "at --prec bits, host mpfr_t arrays) next to the reference's serial and OpenMP-4 code")
+    ap.add_argument("--dropin-tier", default="mp", choices=["mp", "fp64"],
+                    help="--dropin: mp_sr24_cp_fft (mp) or d_sr24_cp_fft on host double arrays (fp64)")
     return ap.parse_args()
 
 
@@ -215,6 +217,9 @@ def dropin_arm(args):
     from mpfft_b200 import mparray
     from oracle import oracle as O
 
+    if args.dropin_tier == "fp64":
+        dropin_fp64(args)
+        return
     n, p = args.n, args.prec
     xr, xi = mparray.MpfrArray(n, p), mparray.MpfrArray(n, p)
     mparray.fill_uniform(xr, xi, SEED)
@@ -239,6 +244,58 @@ def dropin_arm(args):
                       "value": us, "unit": "us", "higher_is_better": False, "calls_per_s": 1e6 / us,
                       "config": {"n": n, "prec_bits": p, "calls": reps},
                       "reference_serial_us": ser, "reference_omp4_us": omp,
+                      "speedup_vs_serial": (ser / us) if ser else None}))
+
+
+def dropin_fp64(args):
+    """One signal per d_sr24_cp_fft call (host double arrays, copies and
+    synchronisation inside each call), the same transform on device-resident
+    data (one signal per launch sequence, CUDA events), and the reference's
+    serial double code (lab/serial/double/serial_d_fft6.c) on the host."""
+    import numpy as np
+    import torch
+
+    import mpfft_b200 as M
+    from oracle import oracle as O
+
+    n = args.n
+    rng = np.random.default_rng(SEED)
+    xr, xi = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    yr, yi = np.zeros(n), np.zeros(n)
+    for _ in range(10):
+        if M.d_sr24_cp_fft(n, 1, 0, xr, xi, yr, yi) != M.OK:
+            raise RuntimeError(M.last_error())
+    reps = max(20, min(300, int(3e7 / n)))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        M.d_sr24_cp_fft(n, 1, 0, xr, xi, yr, yi)
+    us = (time.perf_counter() - t0) / reps * 1e6
+    plan = M.DPlan(n)
+    d_in = torch.from_numpy(np.concatenate([xr, xi])).cuda()
+    d_out = torch.empty_like(d_in)
+    st = torch.cuda.current_stream()
+    for _ in range(10):
+        plan.execute_device(1, d_in.data_ptr(), d_out.data_ptr(), stream=st.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(reps):
+        plan.execute_device(1, d_in.data_ptr(), d_out.data_ptr(), stream=st.cuda_stream)
+    e1.record(st)
+    torch.cuda.synchronize()
+    dev_us = e0.elapsed_time(e1) / reps * 1e3
+    ser = None
+    if O.ref_available("d6"):
+        ref = O.Ref("d6", n)
+        ref.d_view(0)[:] = xr
+        ref.d_view(1)[:] = xi
+        t1 = ref.run(3)[0] / 3
+        m = max(3, int(1e9 / max(t1, 1)))
+        ser = ref.run(m)[0] / m / 1e3
+        ref.free()
+    print(json.dumps({"metric": "drop-in call latency: one signal per d_sr24_cp_fft call, host double arrays",
+                      "value": us, "unit": "us", "higher_is_better": False, "config": {"n": n, "calls": reps},
+                      "device_resident_us": dev_us, "reference_serial_us": ser,
                       "speedup_vs_serial": (ser / us) if ser else None}))
 
 

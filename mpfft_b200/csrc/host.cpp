@@ -320,6 +320,13 @@ static inline void stage_limbs(uint64_t *dst, const uint64_t *src, int words) {
   memcpy(dst, src, (size_t)words * 8);
 }
 
+// Host copies of large arrays of doubles (to and from pinned staging) on the
+// worker pool, 512 KB per piece; small copies stay on the calling thread.
+constexpr long kParCopyGrain = 1L << 16;
+static void par_copy(double *dst, const double *src, size_t n) {
+  parallel_for((long)n, kParCopyGrain, [&](long a, long b) { memcpy(dst + a, src + a, (size_t)(b - a) * sizeof(double)); });
+}
+
 static inline void stage_word(int64_t *dst, int64_t v) {
 #if defined(__x86_64__)
   _mm_stream_si64(reinterpret_cast<long long *>(dst), (long long)v);
@@ -1361,21 +1368,23 @@ static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *in
   const size_t cim = (size_t)N * batch;
   // [c][b][p]: each signal contiguous
   if (s == 1) {
-    memcpy(p->h_in, inr, cim * sizeof(double));
-    memcpy(p->h_in + cim, ini, cim * sizeof(double));
+    par_copy(p->h_in, inr, cim);
+    par_copy(p->h_in + cim, ini, cim);
   } else {
-    for (size_t t = 0; t < cim; ++t) {
-      p->h_in[t] = inr[t * s];
-      p->h_in[cim + t] = ini[t * s];
-    }
+    parallel_for((long)cim, kParCopyGrain, [&](long t0, long t1) {
+      for (long t = t0; t < t1; ++t) {
+        p->h_in[t] = inr[(size_t)t * s];
+        p->h_in[cim + t] = ini[(size_t)t * s];
+      }
+    });
   }
   const size_t bytes = 2 * cim * sizeof(double);
   CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, bytes, cudaMemcpyHostToDevice, p->stream));
   CUDA_TRY(d_transform(p, p->d_in, p->d_out, (int)batch, flags, p->stream, tmp));
   CUDA_TRY(cudaMemcpyAsync(p->h_out, p->d_out, bytes, cudaMemcpyDeviceToHost, p->stream));
   CUDA_TRY(cudaStreamSynchronize(p->stream));
-  memcpy(outr, p->h_out, cim * sizeof(double));
-  memcpy(outi, p->h_out + cim, cim * sizeof(double));
+  par_copy(outr, p->h_out, cim);
+  par_copy(outi, p->h_out + cim, cim);
   return set_err(MPFFT_OK, "");
 }
 
@@ -1487,11 +1496,11 @@ static int d_execute_real(mpfft_d_plan *p, bool forward, unsigned long batch, co
     CUDA_TRY(d_real_split(true, p->d_out, tmp, (int)M, (int)batch, p->d_wc, p->d_ws, scale, p->stream));
     CUDA_TRY(cudaMemcpyAsync(p->h_out, tmp, 2 * H * batch * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
     CUDA_TRY(cudaStreamSynchronize(p->stream));
-    memcpy(outr, p->h_out, H * batch * sizeof(double));
-    memcpy(outi, p->h_out + H * batch, H * batch * sizeof(double));
+    par_copy(outr, p->h_out, H * batch);
+    par_copy(outi, p->h_out + H * batch, H * batch);
   } else {
-    memcpy(p->h_in, inr, H * batch * sizeof(double));
-    memcpy(p->h_in + H * batch, ini, H * batch * sizeof(double));
+    par_copy(p->h_in, inr, H * batch);
+    par_copy(p->h_in + H * batch, ini, H * batch);
     CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, 2 * H * batch * sizeof(double), cudaMemcpyHostToDevice, p->stream));
     CUDA_TRY(d_real_split(false, p->d_in, tmp, (int)M, (int)batch, p->d_wc, p->d_ws, 1.0, p->stream));
     CUDA_TRY(d_run_transform(p->tabs, tmp, p->d_out, (int)batch, scale, p->stream));
@@ -1833,13 +1842,13 @@ MPFFT_API int mpfft_dd_execute(mpfft_d_plan *plan, unsigned long batch, const do
   if (int e = d_reserve(plan, batch)) return e;
   const size_t pl = (size_t)plan->N * batch;
   const double *src[4] = {xr_hi, xr_lo, xi_hi, xi_lo};
-  for (int i = 0; i < 4; ++i) memcpy(plan->h_in + i * pl, src[i], pl * sizeof(double));
+  for (int i = 0; i < 4; ++i) par_copy(plan->h_in + i * pl, src[i], pl);
   CUDA_TRY(cudaMemcpyAsync(plan->d_in, plan->h_in, 4 * pl * sizeof(double), cudaMemcpyHostToDevice, plan->stream));
   CUDA_TRY(dd_run_transform(plan->tabs, plan->d_in, plan->d_out, (int)batch, d_scale(plan, flags), plan->stream));
   CUDA_TRY(cudaMemcpyAsync(plan->h_out, plan->d_out, 4 * pl * sizeof(double), cudaMemcpyDeviceToHost, plan->stream));
   CUDA_TRY(cudaStreamSynchronize(plan->stream));
   double *dst[4] = {yr_hi, yr_lo, yi_hi, yi_lo};
-  for (int i = 0; i < 4; ++i) memcpy(dst[i], plan->h_out + i * pl, pl * sizeof(double));
+  for (int i = 0; i < 4; ++i) par_copy(dst[i], plan->h_out + i * pl, pl);
   return set_err(MPFFT_OK, "");
 }
 
