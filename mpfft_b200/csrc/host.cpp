@@ -323,6 +323,7 @@ static inline void stage_limbs(uint64_t *dst, const uint64_t *src, int words) {
 // Host copies of large arrays of doubles (to and from pinned staging) on the
 // worker pool, 512 KB per piece; small copies stay on the calling thread.
 constexpr long kParCopyGrain = 1L << 16;
+constexpr size_t kCopyPiece = (size_t)1 << 18;  // doubles (2 MB) per overlapped staging piece
 static void par_copy(double *dst, const double *src, size_t n) {
   parallel_for((long)n, kParCopyGrain, [&](long a, long b) { memcpy(dst + a, src + a, (size_t)(b - a) * sizeof(double)); });
 }
@@ -508,7 +509,9 @@ struct mpfft_d_plan {
   std::mutex mu;
   size_t cap = 0;
   double *d_in = nullptr, *d_out = nullptr, *h_in = nullptr, *h_out = nullptr;
+  std::vector<cudaEvent_t> piece_done;  // chunked device-to-host copies (d_execute_impl)
   ~mpfft_d_plan() {
+    for (cudaEvent_t e : piece_done) cudaEventDestroy(e);
     for (void *q : dev_allocs) cudaFree(q);
     if (d_wr) cudaFree(d_wr);
     if (d_wi) cudaFree(d_wi);
@@ -1367,6 +1370,40 @@ static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *in
   const unsigned long N = p->N;
   const size_t cim = (size_t)N * batch;
   // [c][b][p]: each signal contiguous
+  const size_t bytes = 2 * cim * sizeof(double);
+  if (s == 1 && 2 * cim > kCopyPiece) {
+    // large arrays: pieces of the staging copies overlap the PCIe transfers
+    // (piece i is copied into pinned memory while piece i-1 is in flight, and
+    // copied out of it once its transfer has landed)
+    const size_t total = 2 * cim, np = (total + kCopyPiece - 1) / kCopyPiece;
+    while (p->piece_done.size() < np) {
+      cudaEvent_t e;
+      CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      p->piece_done.push_back(e);
+    }
+    // element o of the concatenated [re | im] staging lives in re[o] or im[o - cim]
+    auto each_part = [&](size_t o, size_t len, const std::function<void(size_t, size_t, size_t)> &fn) {
+      if (o < cim) fn(o, o, std::min(len, cim - o));
+      if (o + len > cim) fn(std::max(o, cim), std::max(o, cim) - cim, o + len - std::max(o, cim));
+    };
+    for (size_t i = 0; i < np; ++i) {
+      const size_t o = i * kCopyPiece, len = std::min(kCopyPiece, total - o);
+      each_part(o, len, [&](size_t at, size_t src, size_t cnt) { par_copy(p->h_in + at, (at < cim ? inr : ini) + src, cnt); });
+      CUDA_TRY(cudaMemcpyAsync(p->d_in + o, p->h_in + o, len * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    }
+    CUDA_TRY(d_transform(p, p->d_in, p->d_out, (int)batch, flags, p->stream, tmp));
+    for (size_t i = 0; i < np; ++i) {
+      const size_t o = i * kCopyPiece, len = std::min(kCopyPiece, total - o);
+      CUDA_TRY(cudaMemcpyAsync(p->h_out + o, p->d_out + o, len * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+      CUDA_TRY(cudaEventRecord(p->piece_done[i], p->stream));
+    }
+    for (size_t i = 0; i < np; ++i) {
+      const size_t o = i * kCopyPiece, len = std::min(kCopyPiece, total - o);
+      CUDA_TRY(cudaEventSynchronize(p->piece_done[i]));
+      each_part(o, len, [&](size_t at, size_t dst, size_t cnt) { par_copy((at < cim ? outr : outi) + dst, p->h_out + at, cnt); });
+    }
+    return set_err(MPFFT_OK, "");
+  }
   if (s == 1) {
     par_copy(p->h_in, inr, cim);
     par_copy(p->h_in + cim, ini, cim);
@@ -1378,7 +1415,6 @@ static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *in
       }
     });
   }
-  const size_t bytes = 2 * cim * sizeof(double);
   CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, bytes, cudaMemcpyHostToDevice, p->stream));
   CUDA_TRY(d_transform(p, p->d_in, p->d_out, (int)batch, flags, p->stream, tmp));
   CUDA_TRY(cudaMemcpyAsync(p->h_out, p->d_out, bytes, cudaMemcpyDeviceToHost, p->stream));
