@@ -25,8 +25,13 @@
  * exact and each twiddle product is rounded once, so the normwise error is
  * below the reference's own at the same P.
  *
- * Thread safety: every entry point may be called from any host thread;
- * calls on the same plan are serialised.
+ * Thread safety: every entry point may be called from any host thread and,
+ * for the asynchronous device-layout entries, on any stream.  Host-side work
+ * of calls on the same plan is serialised.  Where a plan keeps internal device
+ * scratch (multi-dimensional plans, large limb counts, real FP64 plans), the
+ * device work of its calls is also ordered: a call's stream first waits on the
+ * GPU for the previous call that used the scratch, so calls on different
+ * streams give the same results as calls made one after another.
  */
 #ifndef MPFFT_B200_H
 #define MPFFT_B200_H
@@ -58,6 +63,16 @@ extern "C" {
 #define MPFFT_PLAN_NO_TENSOR 16u /* plan creation: keep large-precision twiddle products on the integer
                                      pipes (by default 35..260 limbs use int8 tensor-core GEMMs) */
 #define MPFFT_PLAN_TENSOR 32u    /* plan creation: tensor-core twiddle products from 8 limbs up */
+#define MPFFT_PLAN_FLOAT_TIERS 64u /* plan creation: run host-array transforms of precisions up to 200 bits on a
+                                       compensated floating-point tier (see mpfft_mp_plan_form) */
+
+/* the form an mp plan's host-array transforms run in (mpfft_mp_plan_form) */
+#define MPFFT_FORM_LIMBS 0         /* fixed-point 32-bit limbs, integer pipes */
+#define MPFFT_FORM_TENSOR 1        /* fixed-point limbs, twiddle products as int8 tensor-core GEMMs */
+#define MPFFT_FORM_FLOAT_FLOAT 2   /* float pairs, additions on the FP32 pipe, products in FP64 (P <= 40) */
+#define MPFFT_FORM_DOUBLE 3        /* the reference's double transform (40 < P <= 48) */
+#define MPFFT_FORM_DOUBLE_DOUBLE 4 /* double-double (48 < P <= 98) */
+#define MPFFT_FORM_QUAD_DOUBLE 5   /* quad-double (98 < P <= 200) */
 
 /* ------------------------------------------------------------------------ */
 /* 1. drop-in replacements for mpFFT.h                                      */
@@ -142,6 +157,14 @@ int mpfft_mp_plan_create_nd(mpfft_mp_plan **plan, int rank, const unsigned long 
 int mpfft_mp_plan_destroy(mpfft_mp_plan *plan);
 /* device format of a plan: limbs per real component, fraction bits */
 int mpfft_mp_plan_limbs(const mpfft_mp_plan *plan);
+/* MPFFT_FORM_* of the plan's host-array transforms.  A plan created with
+ * MPFFT_PLAN_FLOAT_TIERS whose precision a compensated floating-point tier
+ * covers (normwise error within 8 log2(n) 2^-P, measured against the 2P-bit
+ * oracle) converts mpfr_t values to that tier's words on the host and runs the
+ * tier's kernels; calls whose inputs lie outside the tier's exponent window
+ * run on the limbs instead.  The device-layout entry points always take limb
+ * planes.  No counterpart in the reference. */
+int mpfft_mp_plan_form(const mpfft_mp_plan *plan);
 long mpfft_mp_plan_frac_bits(const mpfft_mp_plan *plan);
 
 /* Transform `batch` signals held in host mpfr_t arrays: signal b occupies
@@ -220,6 +243,28 @@ int mpfft_dd_execute(mpfft_d_plan *plan, unsigned long batch, const double *xr_h
 int mpfft_dd_execute_device(mpfft_d_plan *plan, unsigned long batch, const double *d_in, double *d_out,
                             unsigned flags, void *stream);
 
+/* Quad-double tier (about 212 bits; no counterpart in the reference): values
+ * x0 + x1 + x2 + x3 of four doubles, each at most half an ulp of the one above;
+ * additions and products summed order by order with error-free
+ * transformations and renormalised (Hida, Li and Bailey's quad-double
+ * algorithms).  Normwise error about log2(n) 2^-209.  Float-float tier (about
+ * 48 bits): values hi + lo of two floats; additions on the FP32 pipe, every
+ * twiddle product formed and renormalised in FP64.  Both take the layout of
+ * the multiword entries below. */
+int mpfft_qd_plan_create(mpfft_d_plan **plan, unsigned long n);
+int mpfft_ff_plan_create(mpfft_d_plan **plan, unsigned long n);
+/* Words per real component (K: 2 double-double, 4 quad-double, 2 float-float)
+ * and bytes per word (8, or 4 for float-float) of a multiword plan. */
+int mpfft_multiword_format(const mpfft_d_plan *plan, int *words, int *word_bytes);
+/* Multiword plans (double-double, quad-double, float-float): word h of the
+ * real (c = 0) or imaginary (c = 1) part of point p of signal b at index
+ * ((c*K + h)*batch + b)*n + p of x / y (host arrays; the same layout on the
+ * device).  flags: MPFFT_SCALED, MPFFT_INVERSE.  The host entry is
+ * synchronous; the device entry is asynchronous on `stream`. */
+int mpfft_multiword_execute(mpfft_d_plan *plan, unsigned long batch, const void *x, void *y, unsigned flags);
+int mpfft_multiword_execute_device(mpfft_d_plan *plan, unsigned long batch, const void *d_in, void *d_out,
+                                   unsigned flags, void *stream);
+
 /* FP64 real transforms of n real points (n a power of two >= 2; no
  * counterpart in the reference): the n/2-point complex transform (the
  * reference's, bit-identical) plus one split step in double.  r2c: in[b*n + j]
@@ -258,7 +303,9 @@ int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, const double
  * per component, least significant first, normalised as in an mpfr_t),
  * exponents (value = sign * 0.significand * 2^exp; INT64_MIN marks zero) and
  * signs (1 = negative).  Outputs are rounded to nearest-even at prec_out bits,
- * as mpfr_set_z_2exp would.  Inputs must be finite.  flags: MPFFT_SCALED.
+ * as mpfr_set_z_2exp would.  Inputs must be finite.  flags: MPFFT_SCALED (any
+ * other flag is rejected with MPFFT_EINVAL).  The current device must be the
+ * one the plan was created on (else MPFFT_EINVAL).
  *
  * Working storage is one static device array of mpfft_static_scratch_bytes()
  * (64 MiB) that every GPU loading this library holds until the process exits:
@@ -301,6 +348,21 @@ int mpfft_diag_tc_mul(int limbs, unsigned long batch, const uint32_t *d_x, const
 /* MPFFT_OK, or MPFFT_ECUDA if a bounded wait of a tensor-core kernel expired
  * since the last call (the synchronous host-array calls check this themselves). */
 int mpfft_diag_tc_error(void);
+/* Limit, in nanoseconds, of each wait of the tensor-core kernels on their own
+ * MMAs (default 2e9).  For tests of the expiry path: with 0 every wait gives
+ * up at once, the kernel drains its MMAs and returns, and the call reports
+ * MPFFT_ECUDA; restore the default afterwards. */
+int mpfft_diag_tc_set_wait_limit(unsigned long long ns);
+/* Fault injection for tests of the MPFFT_ENOMEM paths: the after-th device or
+ * pinned-host allocation of execution buffers from now on (0 = the next one)
+ * and every later one fail as cudaMalloc would; after < 0 switches this off. */
+int mpfft_diag_fail_allocations(long after);
+/* Real multiplications and additions of one transform, counted from the
+ * plan's own schedule (its leaves and levels) with the per-butterfly counts of
+ * the kernels: the reference's op counters (fft_complexity,
+ * lab/parallel/mp/parallel_mp_fft2.c:332-354) give 7172 and 27652 at n = 1024
+ * (lab/serial/mp/OPTIONS.md:42).  One-dimensional complex plans. */
+int mpfft_mp_plan_counts(const mpfft_mp_plan *plan, unsigned long *mults, unsigned long *adds);
 
 #ifdef __cplusplus
 }

@@ -30,6 +30,8 @@ PLAN_HOST_CONVERSION = 4
 INVERSE = 8
 PLAN_NO_TENSOR = 16
 PLAN_TENSOR = 32
+PLAN_FLOAT_TIERS = 64
+FORM_LIMBS, FORM_TENSOR, FORM_FLOAT_FLOAT, FORM_DOUBLE, FORM_DOUBLE_DOUBLE, FORM_QUAD_DOUBLE = range(6)
 
 
 class MpfftError(RuntimeError):
@@ -96,6 +98,15 @@ def _load() -> C.CDLL:
         "mpfft_mp_execute_significands_static": (C.c_int, [vp, ul, vp, vp, vp, C.c_int, vp, vp, vp, sl, C.c_uint,
                                                            vp]),
         "mpfft_static_scratch_bytes": (C.c_size_t, []),
+        "mpfft_diag_tc_set_wait_limit": (C.c_int, [C.c_ulonglong]),
+        "mpfft_diag_fail_allocations": (C.c_int, [C.c_long]),
+        "mpfft_mp_plan_counts": (C.c_int, [vp, C.POINTER(C.c_ulong), C.POINTER(C.c_ulong)]),
+        "mpfft_mp_plan_form": (C.c_int, [vp]),
+        "mpfft_qd_plan_create": (C.c_int, [C.POINTER(vp), ul]),
+        "mpfft_ff_plan_create": (C.c_int, [C.POINTER(vp), ul]),
+        "mpfft_multiword_format": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "mpfft_multiword_execute": (C.c_int, [vp, ul, vp, vp, C.c_uint]),
+        "mpfft_multiword_execute_device": (C.c_int, [vp, ul, vp, vp, C.c_uint, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -179,12 +190,14 @@ class MpPlan:
     """Multiprecision plan for n points at `prec` bits (device limb format)."""
 
     def __init__(self, n: int, prec: int, host_only: bool = False, host_conversion: bool = False,
-                 tensor=True):
+                 tensor=True, float_tiers: bool = False):
         """tensor: True (default choice), False (integer pipes only) or
-        "force" (tensor-core products from 8 limbs up)."""
+        "force" (tensor-core products from 8 limbs up).  float_tiers: run
+        precisions a compensated floating-point tier covers on that tier."""
         h = C.c_void_p()
         flags = ((PLAN_HOST_ONLY if host_only else 0) | (PLAN_HOST_CONVERSION if host_conversion else 0)
-                 | (PLAN_TENSOR if tensor == "force" else 0 if tensor else PLAN_NO_TENSOR))
+                 | (PLAN_TENSOR if tensor == "force" else 0 if tensor else PLAN_NO_TENSOR)
+                 | (PLAN_FLOAT_TIERS if float_tiers else 0))
         _check(lib.mpfft_mp_plan_create_flags(C.byref(h), n, prec, flags))
         self.h = h
         self.n, self.prec = n, prec
@@ -208,6 +221,16 @@ class MpPlan:
 
     def execute_device(self, batch, d_in: int, d_out: int, stream: int = 0) -> None:
         _check(lib.mpfft_mp_execute_device(self.h, batch, d_in, d_out, stream or None))
+
+    def form(self) -> int:
+        """FORM_* of the plan's host-array transforms."""
+        return lib.mpfft_mp_plan_form(self.h)
+
+    def counts(self) -> tuple[int, int]:
+        """(real multiplications, real additions) of one transform, from the plan's schedule."""
+        m, a = C.c_ulong(), C.c_ulong()
+        _check(lib.mpfft_mp_plan_counts(self.h, C.byref(m), C.byref(a)))
+        return m.value, a.value
 
     def schedule(self) -> list[tuple[int, int]]:
         """[(node size n, node count)] of each butterfly launch after the leaf launch."""
@@ -301,6 +324,16 @@ def tc_error() -> None:
     _check(lib.mpfft_diag_tc_error())
 
 
+def tc_set_wait_limit(ns: int) -> None:
+    """Limit of the tensor-core kernels' waits on their own MMAs (tests of the expiry path)."""
+    _check(lib.mpfft_diag_tc_set_wait_limit(ns))
+
+
+def fail_allocations(after: int) -> None:
+    """Make the after-th execution-buffer allocation from now on (and later ones) fail; -1: off."""
+    _check(lib.mpfft_diag_fail_allocations(after))
+
+
 def imad_rate(wide: bool = False) -> float:
     """Measured integer multiply-add rate of the current GPU, ops/s."""
     v = C.c_double()
@@ -381,3 +414,27 @@ class DPlanND(DPlan):
         self.n = 1
         for v in dims:
             self.n *= v
+
+
+class MultiwordPlan(DPlan):
+    """Compensated floating-point tier plan for n points: "dd" (double-double),
+    "qd" (quad-double) or "ff" (float-float).  Arrays: numpy / device buffers in
+    the layout [c][h][b][p] (c re/im, h word), float64 (float32 for "ff")."""
+
+    def __init__(self, n: int, tier: str):
+        h = C.c_void_p()
+        create = {"dd": lib.mpfft_dd_plan_create, "qd": lib.mpfft_qd_plan_create, "ff": lib.mpfft_ff_plan_create}
+        _check(create[tier](C.byref(h), n))
+        self.h = h
+        self.n, self.tier = n, tier
+        k, wb = C.c_int(), C.c_int()
+        _check(lib.mpfft_multiword_format(h, C.byref(k), C.byref(wb)))
+        self.words, self.word_bytes = k.value, wb.value
+
+    def execute(self, batch, x, y, scaled=False, inverse=False) -> None:
+        flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
+        _check(lib.mpfft_multiword_execute(self.h, batch, _dp(x), _dp(y), flags))
+
+    def execute_device(self, batch, d_in: int, d_out: int, scaled=False, stream: int = 0, inverse=False) -> None:
+        flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
+        _check(lib.mpfft_multiword_execute_device(self.h, batch, d_in, d_out, flags, stream or None))

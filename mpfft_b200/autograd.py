@@ -1,4 +1,4 @@
-"""Differentiable FP64 conjugate-pair FFT for PyTorch.
+"""Differentiable conjugate-pair FFTs for PyTorch: the FP64 and double-double tiers.
 
 The transform y = F x is linear, so its vector-Jacobian product is the
 adjoint: for a real loss L of (Re y, Im y) with cotangent g = dL/dRe y +
@@ -7,16 +7,26 @@ library computes on the device as the unscaled inverse (its first launch reads
 the real and imaginary planes exchanged and its last writes them exchanged).
 No intermediate is saved: the backward pass needs only the plan.
 
-Tensors use the library's FP64 device layout: float64 CUDA tensors of shape
-(2, B, n), all real parts (signal after signal), then all imaginary parts.
+Tensors use the library's device layouts.  FP64: float64 CUDA tensors of
+shape (2, B, n), all real parts (signal after signal), then all imaginary
+parts.  Double-double: shape (2, 2, B, n), [re, im] x [hi, lo].
+
+Double-double cotangents are double-double numbers too: the gradient handed
+to the backward pass for y is read as hi + lo per component (the value of
+dL/dy to about 2^-104 relative), and the gradient returned for x is dL/dx as a
+(hi, lo) pair, computed by the adjoint transform in double-double arithmetic.
+A caller that forms the cotangent in plain float64 (hi only, lo zero) gets a
+float64-accurate gradient; one that forms it in double-double gets a
+double-double one.
 """
 from __future__ import annotations
 
 import torch
 
-from . import DPlan, DPlanND
+from . import DDPlan, DPlan, DPlanND
 
 _plans: dict = {}
+_dd_plans: dict = {}
 
 
 def _plan(dims):
@@ -62,3 +72,42 @@ def fft(z: torch.Tensor, inverse: bool = False, ndim: int = 1) -> torch.Tensor:
     planes = torch.stack((zz.real, zz.imag)).reshape((2, zz.shape[0], -1))
     y = ConjugatePairFFT.apply(planes, dims, inverse)
     return torch.complex(y[0], y[1]).reshape(lead + dims)
+
+
+def _dd_plan(n: int):
+    if n not in _dd_plans:
+        _dd_plans[n] = DDPlan(n)
+    return _dd_plans[n]
+
+
+class DDConjugatePairFFT(torch.autograd.Function):
+    """Double-double y = FFT(x) on planes (2, 2, B, n) = [re, im] x [hi, lo];
+    backward = the adjoint in double-double (the unscaled inverse on the
+    device: planes exchanged in the first and the last launch)."""
+
+    @staticmethod
+    def forward(ctx, x: torch.Tensor, inverse: bool):
+        if x.dtype != torch.float64 or not x.is_cuda or x.dim() != 4 or x.shape[:2] != (2, 2):
+            raise TypeError("expected a float64 CUDA tensor of shape (2, 2, B, n)")
+        x = x.contiguous()
+        batch, n = x.shape[2], x.shape[3]
+        y = torch.empty_like(x)
+        s = torch.cuda.current_stream().cuda_stream
+        _dd_plan(n).execute_device(batch, x.data_ptr(), y.data_ptr(), stream=s, inverse=inverse)
+        ctx.inverse = inverse
+        return y
+
+    @staticmethod
+    def backward(ctx, gy: torch.Tensor):
+        gy = gy.contiguous()
+        gx = torch.empty_like(gy)
+        s = torch.cuda.current_stream().cuda_stream
+        _dd_plan(gy.shape[3]).execute_device(gy.shape[2], gy.data_ptr(), gx.data_ptr(), stream=s,
+                                             inverse=not ctx.inverse)
+        return gx, None
+
+
+def dd_fft(x: torch.Tensor, inverse: bool = False) -> torch.Tensor:
+    """Differentiable double-double transform of planes (2, 2, B, n) = [re, im]
+    x [hi, lo] (n a power of two), unscaled in both directions."""
+    return DDConjugatePairFFT.apply(x, inverse)

@@ -70,6 +70,39 @@ static int set_err(int code, const char *fmt, ...) {
       return set_err(MPFFT_ECUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
 
+// ---------------------------------------------------------------------------
+// allocations of execution buffers, with a test hook
+// ---------------------------------------------------------------------------
+// Every device or pinned-host buffer that an execution grows on demand comes
+// from these two functions.  mpfft_diag_fail_allocations(k) makes the k-th
+// such allocation from now on (0 = the next one), and every later one, fail as
+// cudaMalloc would, so that the MPFFT_ENOMEM paths can be exercised without
+// exhausting a real device; -1 switches the hook off.
+static std::atomic<long> g_alloc_fail_after{-1};
+
+static bool alloc_should_fail() {
+  long v = g_alloc_fail_after.load();
+  while (v > 0 && !g_alloc_fail_after.compare_exchange_weak(v, v - 1)) {
+  }
+  return v == 0;
+}
+
+static cudaError_t dev_alloc(void **p, size_t bytes) {
+  if (alloc_should_fail()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
+static cudaError_t host_alloc(void **p, size_t bytes) {
+  if (alloc_should_fail()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocHost(p, bytes);
+}
+
 static bool is_pow2(unsigned long n) { return n >= 1 && (n & (n - 1)) == 0; }
 static int ilog2(unsigned long n) {
   int l = 0;
@@ -113,6 +146,8 @@ static int build_tree(DeviceTree &dt, unsigned long N, int leaf_max) {
   walk(t, (int)N, 1, 0, 0, leaf_max);
   dt.tabs.N = (int)N;
   dt.tabs.nleaves = (int)t.leaves.size();
+  for (const Leaf &lf : t.leaves)
+    if (lf.n <= 4) ++dt.tabs.leaf_count[lf.n];
   std::vector<int> nodes;
   int lv = 0;
   for (auto &kv : t.levels) {
@@ -411,6 +446,10 @@ static int build_twiddles(MpTwiddles &tw, unsigned long N, int L) {
 
 using namespace mpfft;
 
+namespace mpfft {
+static void d_plan_delete(mpfft_d_plan *p);
+}
+
 struct mpfft_mp_plan {
   unsigned long N = 0;
   long P = 0;
@@ -430,6 +469,12 @@ struct mpfft_mp_plan {
   size_t tmp_words = 0;
   uint32_t *d_big = nullptr;  // streaming-kernel scratch (L > kMaxLimbs), grown on demand
   size_t big_words = 0;
+  // Device work that reads or writes d_tmp / d_big is ordered across calls:
+  // each such call makes its stream wait for scratch_ev (recorded after the
+  // previous such call's kernels) and records it again after its own, under mu.
+  cudaEvent_t scratch_ev = nullptr;
+  bool scratch_recorded = false;
+  int device = -1;  // the CUDA device the plan's tables live on (-1: host-only plan)
   DeviceTree tree;
   MpTwiddles tw;
   MpDeviceTables tabs;
@@ -476,8 +521,15 @@ struct mpfft_mp_plan {
     }
     cv_chunk = 0;
   }
+  // MPFFT_PLAN_FLOAT_TIERS: the compensated floating-point plan that runs this
+  // plan's host-array transforms (null: the limb kernels run them), and the
+  // form the plan reports (MPFFT_FORM_*)
+  mpfft_d_plan *fplan = nullptr;
+  int form = MPFFT_FORM_LIMBS;
   ~mpfft_mp_plan() {
     free_conv();
+    d_plan_delete(fplan);
+    if (scratch_ev) cudaEventDestroy(scratch_ev);
     if (d_tmp) cudaFree(d_tmp);
     if (d_big) cudaFree(d_big);
     if (d_in) cudaFree(d_in);
@@ -496,8 +548,10 @@ struct mpfft_d_plan {
   std::unique_ptr<mpfft_d_plan> axis[3];
   double *d_tmp = nullptr;  // rank > 1: transposition buffer; real plans: split-step output
   size_t tmp_cap = 0;
-  bool dd = false;          // double-double tier (dd_kernels.cu)
-  double *d_wrl = nullptr, *d_wil = nullptr;
+  cudaEvent_t scratch_ev = nullptr;  // orders the device work that uses d_tmp across calls (as mp plans)
+  bool scratch_recorded = false;
+  bool dd = false;          // double-double tier
+  int tier = -1;            // compensated tier (kTierDD / kTierQD / kTierFF), -1 for FP64
   bool real = false;        // real transform of n_real = 2N points: N-point complex transform + split step
   unsigned long n_real = 0;
   double *d_wc = nullptr, *d_ws = nullptr;  // real plans: cos, sin of 2 pi k / n_real, k < N/2
@@ -511,6 +565,7 @@ struct mpfft_d_plan {
   double *d_in = nullptr, *d_out = nullptr, *h_in = nullptr, *h_out = nullptr;
   std::vector<cudaEvent_t> piece_done;  // chunked device-to-host copies (d_execute_impl)
   ~mpfft_d_plan() {
+    if (scratch_ev) cudaEventDestroy(scratch_ev);
     for (cudaEvent_t e : piece_done) cudaEventDestroy(e);
     for (void *q : dev_allocs) cudaFree(q);
     if (d_wr) cudaFree(d_wr);
@@ -521,8 +576,6 @@ struct mpfft_d_plan {
     if (h_out) cudaFreeHost(h_out);
     if (d_tmp) cudaFree(d_tmp);
     if (d_wc) cudaFree(d_wc);
-    if (d_wrl) cudaFree(d_wrl);
-    if (d_wil) cudaFree(d_wil);
     if (d_ws) cudaFree(d_ws);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -535,6 +588,24 @@ static int device_ready() {
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0)
     return set_err(MPFFT_ECUDA, "no CUDA device available: %s", cudaGetErrorString(e));
+  return MPFFT_OK;
+}
+
+// Device work that uses a plan's shared scratch is ordered across calls and
+// streams: the call's stream first waits for the previous such call's kernels
+// (scratch_ev), and the event is recorded again after the call's own kernels.
+// The caller holds the plan's lock from scratch_wait to scratch_record.
+template <class Plan>
+static int scratch_wait(Plan *p, cudaStream_t st) {
+  if (!p->scratch_ev) CUDA_TRY(cudaEventCreateWithFlags(&p->scratch_ev, cudaEventDisableTiming));
+  if (p->scratch_recorded) CUDA_TRY(cudaStreamWaitEvent(st, p->scratch_ev, 0));
+  return MPFFT_OK;
+}
+
+template <class Plan>
+static int scratch_record(Plan *p, cudaStream_t st) {
+  CUDA_TRY(cudaEventRecord(p->scratch_ev, st));
+  p->scratch_recorded = true;
   return MPFFT_OK;
 }
 
@@ -565,6 +636,7 @@ static int mp_plan_init(mpfft_mp_plan *p, unsigned long n, long prec, bool host_
   p->host_only = host_only;
   if (host_only) return MPFFT_OK;
   if (int e = device_ready()) return e;
+  CUDA_TRY(cudaGetDevice(&p->device));
   if (int e = build_tree(p->tree, nt, 4)) return e;
   if (int e = build_twiddles(p->tw, n, L)) return e;
   static_cast<TreeTables &>(p->tabs) = p->tree.tabs;
@@ -594,12 +666,49 @@ static int mp_plan_init_nd(mpfft_mp_plan *p, int rank, const unsigned long *dims
   for (int i = 0; i < rank; ++i) p->dims[i] = dims[i];
   if (host_only) return MPFFT_OK;
   if (int e = device_ready()) return e;
+  CUDA_TRY(cudaGetDevice(&p->device));
   for (int i = 0; i < rank; ++i) {
     p->axis[i].reset(new (std::nothrow) mpfft_mp_plan);
     if (!p->axis[i]) return set_err(MPFFT_ENOMEM, "out of host memory");
     if (int e = mp_plan_init(p->axis[i].get(), dims[i], prec, false, false, p->L)) return e;
   }
   CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  return MPFFT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// dispatch of mp plans to the compensated floating-point tiers
+// ---------------------------------------------------------------------------
+//
+// With MPFFT_PLAN_FLOAT_TIERS an mp plan whose precision a floating tier
+// covers runs its host-array transforms on that tier instead of fixed-point
+// limbs.  A tier covers P when its normwise error, measured against the 2P-bit
+// oracle over N = 2 .. 2^16, stays within the mp contract 8 log2(N) 2^-P:
+//   float-float (about 48 bits)  P <= 40
+//   FP64 (the reference's double transform)  40 < P <= 48
+//   double-double (about 106 bits)  48 < P <= 98
+//   quad-double (about 212 bits)  98 < P <= 200
+// Larger precisions keep the limb kernels.
+static int float_form_for(long P) {
+  if (P <= 40) return MPFFT_FORM_FLOAT_FLOAT;
+  if (P <= 48) return MPFFT_FORM_DOUBLE;
+  if (P <= 98) return MPFFT_FORM_DOUBLE_DOUBLE;
+  if (P <= 200) return MPFFT_FORM_QUAD_DOUBLE;
+  return -1;
+}
+
+static int d_plan_init(mpfft_d_plan *p, unsigned long n);
+static int d_plan_init_tier(mpfft_d_plan *p, unsigned long n, int tier);
+
+static int mp_plan_attach_float_tier(mpfft_mp_plan *p) {
+  const int form = float_form_for(p->P);
+  if (form < 0 || p->rank > 1 || p->real || p->host_only) return MPFFT_OK;
+  std::unique_ptr<mpfft_d_plan> f(new (std::nothrow) mpfft_d_plan);
+  if (!f) return set_err(MPFFT_ENOMEM, "out of host memory");
+  const int tier = form == MPFFT_FORM_FLOAT_FLOAT ? kTierFF : form == MPFFT_FORM_DOUBLE_DOUBLE ? kTierDD : kTierQD;
+  if (int e = form == MPFFT_FORM_DOUBLE ? d_plan_init(f.get(), p->N) : d_plan_init_tier(f.get(), p->N, tier)) return e;
+  p->fplan = f.release();
+  p->form = form;
   return MPFFT_OK;
 }
 
@@ -630,8 +739,8 @@ static int mp_reserve(mpfft_mp_plan *p, unsigned long batch) {
   if (p->h_out) cudaFreeHost(p->h_out);
   p->d_in = p->d_out = p->h_in = p->h_out = nullptr;
   p->cap_words = 0;
-  if (cudaMalloc(&p->d_in, words * 4) != cudaSuccess || cudaMalloc(&p->d_out, words * 4) != cudaSuccess ||
-      cudaMallocHost(&p->h_in, words * 4) != cudaSuccess || cudaMallocHost(&p->h_out, words * 4) != cudaSuccess) {
+  if (dev_alloc((void **)&p->d_in, words * 4) != cudaSuccess || dev_alloc((void **)&p->d_out, words * 4) != cudaSuccess ||
+      host_alloc((void **)&p->h_in, words * 4) != cudaSuccess || host_alloc((void **)&p->h_out, words * 4) != cudaSuccess) {
     cudaGetLastError();
     return set_err(MPFFT_ENOMEM, "cannot allocate %zu-byte staging buffers", words * 4);
   }
@@ -780,8 +889,8 @@ static int mp_conv_reserve(mpfft_mp_plan *p, unsigned long chunk, int nli, int n
   const size_t comp = (size_t)2 * p->pts_max() * chunk;
   const size_t words = (size_t)2 * p->L * p->pts_max() * chunk;
   bool ok = true;
-  auto dm = [&](void **q, size_t bytes) { ok = ok && cudaMalloc(q, bytes) == cudaSuccess; };
-  auto hm = [&](void **q, size_t bytes) { ok = ok && cudaMallocHost(q, bytes) == cudaSuccess; };
+  auto dm = [&](void **q, size_t bytes) { ok = ok && dev_alloc(q, bytes) == cudaSuccess; };
+  auto hm = [&](void **q, size_t bytes) { ok = ok && host_alloc(q, bytes) == cudaSuccess; };
   for (auto &c : p->cv) {
     ok = ok && cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) == cudaSuccess;
@@ -1036,7 +1145,7 @@ static int mp_big_reserve(mpfft_mp_plan *p, unsigned long batch, uint32_t **out)
     if (p->d_big) cudaFree(p->d_big);
     p->d_big = nullptr;
     p->big_words = 0;
-    if (cudaMalloc(&p->d_big, words * 4) != cudaSuccess) {
+    if (dev_alloc((void **)&p->d_big, words * 4) != cudaSuccess) {
       cudaGetLastError();
       return set_err(MPFFT_ENOMEM, "cannot allocate %zu bytes of scratch", words * 4);
     }
@@ -1055,7 +1164,7 @@ static int mp_tmp_reserve(mpfft_mp_plan *p, unsigned long batch, uint32_t **out)
     if (p->d_tmp) cudaFree(p->d_tmp);
     p->d_tmp = nullptr;
     p->tmp_words = 0;
-    if (cudaMalloc(&p->d_tmp, words * 4) != cudaSuccess) {
+    if (dev_alloc((void **)&p->d_tmp, words * 4) != cudaSuccess) {
       cudaGetLastError();
       return set_err(MPFFT_ENOMEM, "cannot allocate %zu bytes of transposition scratch", words * 4);
     }
@@ -1077,11 +1186,18 @@ static int mp_tc_check(const mpfft_mp_plan *p, int rc) {
 
 static int mp_execute_hostconv(mpfft_mp_plan *p, unsigned long batch, int mode, const IoShape &ii, mpfr_t *inr,
                                mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj);
+constexpr int kFloatOutOfRange = -1;
+static int mp_execute_float(mpfft_mp_plan *p, unsigned long batch, const IoShape &ii, mpfr_t *inr, mpfr_t *ini,
+                            const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj);
 
 static int mp_execute_impl(mpfft_mp_plan *p, unsigned long batch, int mode, const IoShape &ii, mpfr_t *inr,
                            mpfr_t *ini, const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj) {
   if (p->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
   std::lock_guard<std::mutex> g(p->mu);
+  if (p->fplan && mode == kComplex) {
+    const int r = mp_execute_float(p, batch, ii, inr, ini, oo, outr, outi, fadj);
+    if (r != kFloatOutOfRange) return r;
+  }
   if (!p->force_host_conversion) {
     unsigned long done = 0;
     const int r = mp_execute_gpuconv(p, batch, mode, ii, inr, ini, oo, outr, outi, fadj, &done);
@@ -1113,10 +1229,14 @@ static int mp_execute_hostconv(mpfft_mp_plan *p, unsigned long batch, int mode, 
   uint32_t *big = nullptr, *tmp = nullptr;
   if (int e = mp_big_reserve(p, batch, &big)) return e;
   if (int e = mp_tmp_reserve(p, batch, &tmp)) return e;
+  if (big || tmp)
+    if (int e = scratch_wait(p, p->stream)) return e;
   uint32_t *res = nullptr;
   CUDA_TRY(cudaMemcpyAsync(p->d_in, p->h_in, (size_t)2 * p->L * ii.n * batch * 4, cudaMemcpyHostToDevice,
                            p->stream));
   CUDA_TRY(mp_device_pipeline(p, mode, p->d_in, p->d_out, (int)batch, p->stream, big, tmp, &res));
+  if (big || tmp)
+    if (int e = scratch_record(p, p->stream)) return e;
   CUDA_TRY(cudaMemcpyAsync(p->h_out, res, (size_t)2 * p->L * oo.n * batch * 4, cudaMemcpyDeviceToHost, p->stream));
   CUDA_TRY(cudaStreamSynchronize(p->stream));
   if (int e = mp_tc_check(p, MPFFT_OK)) return e;
@@ -1267,8 +1387,14 @@ static mpfft_d_plan *d_cached(unsigned long n) {
   return raw;
 }
 
+// words per real component and bytes per word of a plan's device layout
+static int d_words(const mpfft_d_plan *p) { return p->tier < 0 ? 1 : tier_words(p->tier); }
+static size_t d_word_bytes(const mpfft_d_plan *p) { return p->tier < 0 ? 8 : tier_word_bytes(p->tier); }
+
 static int d_reserve(mpfft_d_plan *p, unsigned long batch) {
-  const size_t words = (size_t)(p->dd ? 4 : 2) * (p->real ? p->N + 1 : p->N) * batch;
+  // in doubles (float-float words take half a double each)
+  const size_t words =
+      ((size_t)2 * d_words(p) * (p->real ? p->N + 1 : p->N) * batch * d_word_bytes(p) + 7) / 8;
   if (words <= p->cap) return MPFFT_OK;
   if (p->d_in) cudaFree(p->d_in);
   if (p->d_out) cudaFree(p->d_out);
@@ -1276,8 +1402,8 @@ static int d_reserve(mpfft_d_plan *p, unsigned long batch) {
   if (p->h_out) cudaFreeHost(p->h_out);
   p->d_in = p->d_out = p->h_in = p->h_out = nullptr;
   p->cap = 0;
-  if (cudaMalloc(&p->d_in, words * 8) != cudaSuccess || cudaMalloc(&p->d_out, words * 8) != cudaSuccess ||
-      cudaMallocHost(&p->h_in, words * 8) != cudaSuccess || cudaMallocHost(&p->h_out, words * 8) != cudaSuccess) {
+  if (dev_alloc((void **)&p->d_in, words * 8) != cudaSuccess || dev_alloc((void **)&p->d_out, words * 8) != cudaSuccess ||
+      host_alloc((void **)&p->h_in, words * 8) != cudaSuccess || host_alloc((void **)&p->h_out, words * 8) != cudaSuccess) {
     cudaGetLastError();
     return set_err(MPFFT_ENOMEM, "cannot allocate %zu-byte staging buffers", words * 8);
   }
@@ -1349,7 +1475,7 @@ static int d_tmp_reserve(mpfft_d_plan *p, unsigned long batch, double **out) {
     if (p->d_tmp) cudaFree(p->d_tmp);
     p->d_tmp = nullptr;
     p->tmp_cap = 0;
-    if (cudaMalloc(&p->d_tmp, words * 8) != cudaSuccess) {
+    if (dev_alloc((void **)&p->d_tmp, words * 8) != cudaSuccess) {
       cudaGetLastError();
       return set_err(MPFFT_ENOMEM, "cannot allocate %zu bytes of transposition scratch", words * 8);
     }
@@ -1367,6 +1493,10 @@ static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *in
   if (int e = d_reserve(p, batch)) return e;
   double *tmp = nullptr;
   if (int e = d_tmp_reserve(p, batch, &tmp)) return e;
+  // wait for device calls still using d_tmp; this call itself holds the lock
+  // until its stream is synchronised, so later callers need no event from it
+  if (tmp)
+    if (int e = scratch_wait(p, p->stream)) return e;
   const unsigned long N = p->N;
   const size_t cim = (size_t)N * batch;
   // [c][b][p]: each signal contiguous
@@ -1424,16 +1554,20 @@ static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *in
   return set_err(MPFFT_OK, "");
 }
 
-// Double-double plan: the same tree, cut at T = min(n, 2048) points, base cases
-// of at most 4 points, twiddles cos/sin(2 pi k/n) rounded to double-double.
-static int d_plan_init_dd(mpfft_d_plan *p, unsigned long n) {
+// Compensated-tier plan (double-double, quad-double, float-float): the same
+// tree, cut at T = min(n, tier_sub_max) points, base cases of at most 4
+// points; cos and sin of 2 pi k/n computed by MPFR at 320 bits and split into
+// the tier's words (each the nearest double to what the words above leave;
+// float-float keeps one double: its products are formed in FP64).
+static int d_plan_init_tier(mpfft_d_plan *p, unsigned long n, int tier) {
   if (!is_pow2(n)) return set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
   if (n > (1UL << 26)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
   if (int e = device_ready()) return e;
   p->N = n;
-  p->dd = true;
+  p->tier = tier;
+  p->dd = tier == kTierDD;
   p->tabs.N = (int)n;
-  const int T = (int)std::min<unsigned long>(n, kDDSubMax);
+  const int T = (int)std::min<unsigned long>(n, (unsigned long)tier_sub_max(tier));
   {
     HostTree t;
     walk(t, (int)n, 1, 0, 0, T);
@@ -1450,42 +1584,43 @@ static int d_plan_init_dd(mpfft_d_plan *p, unsigned long n) {
   } else {
     p->tabs.sub[1] = p->tabs.sub[0];
   }
+  const int K = tier == kTierQD ? 4 : tier == kTierDD ? 2 : 1;  // twiddle words
   const unsigned long q = std::max<unsigned long>(1, n / 4);
-  std::vector<double> ch(q), cl(q), sh(q), sl(q);
+  std::vector<double> w((size_t)2 * K * q);  // [cos words][sin words][k]
   parallel_for((long)q, 64, [&](long a, long b) {
-    mpfr_t th, c, s, r;
-    mpfr_init2(th, 200);
-    mpfr_init2(c, 160);
-    mpfr_init2(s, 160);
-    mpfr_init2(r, 160);
+    mpfr_t th, c, s;
+    mpfr_init2(th, 360);
+    mpfr_init2(c, 320);
+    mpfr_init2(s, 320);
     for (long k = a; k < b; ++k) {
       mpfr_const_pi(th, MPFR_RNDN);
       mpfr_mul_ui(th, th, 2UL * (unsigned long)k, MPFR_RNDN);
       mpfr_div_ui(th, th, n, MPFR_RNDN);
       mpfr_sin_cos(s, c, th, MPFR_RNDN);
-      ch[k] = mpfr_get_d(c, MPFR_RNDN);
-      mpfr_sub_d(r, c, ch[k], MPFR_RNDN);
-      cl[k] = mpfr_get_d(r, MPFR_RNDN);
-      sh[k] = mpfr_get_d(s, MPFR_RNDN);
-      mpfr_sub_d(r, s, sh[k], MPFR_RNDN);
-      sl[k] = mpfr_get_d(r, MPFR_RNDN);
+      for (int h = 0; h < K; ++h) {  // exact remainders at 320 bits
+        w[(size_t)h * q + k] = mpfr_get_d(c, MPFR_RNDN);
+        mpfr_sub_d(c, c, w[(size_t)h * q + k], MPFR_RNDN);
+        w[(size_t)(K + h) * q + k] = mpfr_get_d(s, MPFR_RNDN);
+        mpfr_sub_d(s, s, w[(size_t)(K + h) * q + k], MPFR_RNDN);
+      }
     }
     mpfr_clear(th);
     mpfr_clear(c);
     mpfr_clear(s);
-    mpfr_clear(r);
     mpfr_free_cache();
   });
-  double **dst[4] = {&p->d_wr, &p->d_wrl, &p->d_wi, &p->d_wil};
-  const std::vector<double> *src[4] = {&ch, &cl, &sh, &sl};
-  for (int i = 0; i < 4; ++i) {
-    CUDA_TRY(cudaMalloc(dst[i], q * sizeof(double)));
-    CUDA_TRY(cudaMemcpy(*dst[i], src[i]->data(), q * sizeof(double), cudaMemcpyHostToDevice));
+  const double *dw = nullptr;
+  if (int e = upload(p, w, &dw)) return e;
+  for (int h = 0; h < K; ++h) {
+    p->tabs.tw_cos[h] = dw + (size_t)h * q;
+    p->tabs.tw_sin[h] = dw + (size_t)(K + h) * q;
   }
-  p->tabs.wr = p->d_wr;
-  p->tabs.wrl = p->d_wrl;
-  p->tabs.wi = p->d_wi;
-  p->tabs.wil = p->d_wil;
+  p->tabs.wr = p->tabs.tw_cos[0];
+  p->tabs.wi = p->tabs.tw_sin[0];
+  if (K >= 2) {
+    p->tabs.wrl = p->tabs.tw_cos[1];
+    p->tabs.wil = p->tabs.tw_sin[1];
+  }
   CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   return MPFFT_OK;
 }
@@ -1519,6 +1654,7 @@ static int d_execute_real(mpfft_d_plan *p, bool forward, unsigned long batch, co
   if (int e = d_reserve(p, batch)) return e;
   double *tmp = nullptr;
   if (int e = d_tmp_reserve(p, batch, &tmp)) return e;
+  if (int e = scratch_wait(p, p->stream)) return e;  // the real path always uses d_tmp
   const double scale = (flags & MPFFT_SCALED) ? 1.0 / (double)n : 1.0;
   if (forward) {
     // even samples -> real plane, odd samples -> imaginary plane ([c][b][m])
@@ -1549,6 +1685,87 @@ static int d_execute_real(mpfft_d_plan *p, bool forward, unsigned long batch, co
         xout[b * n + 2 * m + 1] = p->h_out[b * M + m];
       }
   }
+  return set_err(MPFFT_OK, "");
+}
+
+static void d_plan_delete(mpfft_d_plan *p) { delete p; }
+
+// A transform through the plan's compensated floating-point tier: every mpfr_t
+// input is split on the host into the tier's words (the nearest word, then the
+// nearest word to what is left, ...; exact down to the last word), the tier's
+// kernels run, and each output is the words' sum (at 320 bits, exact for
+// these words) times 2^-fadj, rounded to nearest into the output's precision.
+// Returns kFloatOutOfRange, before writing any output, when an input exponent
+// lies outside the window the tier's words represent without underflow or
+// overflow over N-point growth; the caller then runs the limb kernels.
+static int mp_execute_float(mpfft_mp_plan *p, unsigned long batch, const IoShape &ii, mpfr_t *inr, mpfr_t *ini,
+                            const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj) {
+  mpfft_d_plan *f = p->fplan;
+  const unsigned long N = p->N;
+  if ((unsigned long long)batch * N > (unsigned long long)INT32_MAX)
+    return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  std::lock_guard<std::mutex> g(f->mu);
+  if (int e = d_reserve(f, batch)) return e;
+  const int K = d_words(f);
+  const bool fl = d_word_bytes(f) == 4;
+  const long emin = fl ? -100 : -700, emax = fl ? 90 : 900;
+  const size_t hplane = (size_t)N * batch;
+  float *hf = reinterpret_cast<float *>(f->h_in);
+  std::atomic<int> nonfin{0}, range{0};
+  parallel_for((long)hplane, 1024, [&](long a0, long a1) {
+    mpfr_t t;
+    mpfr_init2(t, 64);
+    for (long u = a0; u < a1; ++u) {
+      const unsigned long b = (unsigned long)u / N, q = (unsigned long)u % N;
+      for (int c = 0; c < 2; ++c) {
+        mpfr_srcptr x = elem(c ? ini : inr, c, b, ii, q);
+        const size_t at = ((size_t)c * K * batch + b) * N + q;
+        if (!mpfr_number_p(x)) {
+          nonfin.store(1, std::memory_order_relaxed);
+          continue;
+        }
+        if (!mpfr_zero_p(x) && (x->_mpfr_exp < emin || x->_mpfr_exp > emax)) {
+          range.store(1, std::memory_order_relaxed);
+          continue;
+        }
+        if (mpfr_get_prec(t) < mpfr_get_prec(x)) mpfr_set_prec(t, mpfr_get_prec(x));
+        mpfr_set(t, x, MPFR_RNDN);  // exact
+        for (int h = 0; h < K; ++h) {
+          const double w = fl ? (double)(float)mpfr_get_d(t, MPFR_RNDN) : mpfr_get_d(t, MPFR_RNDN);
+          mpfr_sub_d(t, t, w, MPFR_RNDN);  // exact: the part of t below w
+          if (fl) hf[at + (size_t)h * hplane] = (float)w;
+          else f->h_in[at + (size_t)h * hplane] = w;
+        }
+      }
+    }
+    mpfr_clear(t);
+  });
+  if (range.load()) return kFloatOutOfRange;
+  if (nonfin.load()) return set_err(MPFFT_ENONFINITE, "input holds NaN or infinity");
+  const size_t bytes = (size_t)2 * K * hplane * d_word_bytes(f);
+  CUDA_TRY(cudaMemcpyAsync(f->d_in, f->h_in, bytes, cudaMemcpyHostToDevice, f->stream));
+  if (f->tier < 0) CUDA_TRY(d_run_transform(f->tabs, f->d_in, f->d_out, (int)batch, 1.0, f->stream));
+  else CUDA_TRY(tier_run_transform(f->tier, f->tabs, f->d_in, f->d_out, (int)batch, 1.0, f->stream));
+  CUDA_TRY(cudaMemcpyAsync(f->h_out, f->d_out, bytes, cudaMemcpyDeviceToHost, f->stream));
+  CUDA_TRY(cudaStreamSynchronize(f->stream));
+  const float *of = reinterpret_cast<const float *>(f->h_out);
+  parallel_for((long)hplane, 1024, [&](long a0, long a1) {
+    mpfr_t acc;
+    mpfr_init2(acc, 320);
+    for (long u = a0; u < a1; ++u) {
+      const unsigned long b = (unsigned long)u / N, q = (unsigned long)u % N;
+      for (int c = 0; c < 2; ++c) {
+        const size_t at = ((size_t)c * K * batch + b) * N + q;
+        mpfr_set_zero(acc, 1);
+        for (int h = 0; h < K; ++h)
+          mpfr_add_d(acc, acc, fl ? (double)of[at + (size_t)h * hplane] : f->h_out[at + (size_t)h * hplane],
+                     MPFR_RNDN);
+        mpfr_mul_2si(acc, acc, -fadj, MPFR_RNDN);
+        mpfr_set(elem(c ? outi : outr, c, b, oo, q), acc, MPFR_RNDN);
+      }
+    }
+    mpfr_clear(acc);
+  });
   return set_err(MPFFT_OK, "");
 }
 
@@ -1650,6 +1867,9 @@ MPFFT_API int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, 
   p->force_host_conversion = (flags & MPFFT_PLAN_HOST_CONVERSION) != 0;
   if (flags & MPFFT_PLAN_NO_TENSOR) p->tabs.tc = 0;
   else if (flags & MPFFT_PLAN_TENSOR) p->tabs.tc = 2;
+  if (!p->host_only && mp_tc_used(p->tabs, p->L)) p->form = MPFFT_FORM_TENSOR;
+  if (flags & MPFFT_PLAN_FLOAT_TIERS)
+    if (int e = mp_plan_attach_float_tier(p.get())) return e;
   *plan = p.release();
   return set_err(MPFFT_OK, "");
 }
@@ -1682,6 +1902,7 @@ MPFFT_API int mpfft_mp_plan_destroy(mpfft_mp_plan *plan) {
 }
 
 MPFFT_API int mpfft_mp_plan_limbs(const mpfft_mp_plan *plan) { return plan ? plan->L : 0; }
+MPFFT_API int mpfft_mp_plan_form(const mpfft_mp_plan *plan) { return plan ? plan->form : -1; }
 MPFFT_API long mpfft_mp_plan_frac_bits(const mpfft_mp_plan *plan) { return plan ? plan->F : 0; }
 
 MPFFT_API int mpfft_mp_execute(mpfft_mp_plan *plan, unsigned long batch, mpfr_t *inr, mpfr_t *ini, mpfr_t *outr,
@@ -1815,10 +2036,16 @@ MPFFT_API int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, 
   if (a < b + bytes && b < a + bytes) return set_err(MPFFT_EINVAL, "input and output buffers overlap");
   if (batch > (unsigned long)INT32_MAX || (unsigned long long)batch * plan->N > (unsigned long long)INT32_MAX)
     return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  std::lock_guard<std::mutex> g(plan->mu);
   uint32_t *big = nullptr, *tmp = nullptr;
   if (int e = mp_big_reserve(plan, batch, &big)) return e;
   if (int e = mp_tmp_reserve(plan, batch, &tmp)) return e;
-  CUDA_TRY(mp_transform(plan, d_in, d_out, (int)batch, (cudaStream_t)stream, big, tmp));
+  const cudaStream_t st = (cudaStream_t)stream;
+  if (big || tmp)
+    if (int e = scratch_wait(plan, st)) return e;
+  CUDA_TRY(mp_transform(plan, d_in, d_out, (int)batch, st, big, tmp));
+  if (big || tmp)
+    if (int e = scratch_record(plan, st)) return e;
   return set_err(MPFFT_OK, "");
 }
 
@@ -1854,8 +2081,74 @@ MPFFT_API int mpfft_dd_plan_create(mpfft_d_plan **plan, unsigned long n) {
   *plan = nullptr;
   std::unique_ptr<mpfft_d_plan> p(new (std::nothrow) mpfft_d_plan);
   if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
-  if (int e = d_plan_init_dd(p.get(), n)) return e;
+  if (int e = d_plan_init_tier(p.get(), n, kTierDD)) return e;
   *plan = p.release();
+  return set_err(MPFFT_OK, "");
+}
+
+static int d_plan_create_tier(mpfft_d_plan **plan, unsigned long n, int tier) {
+  if (!plan) return set_err(MPFFT_EINVAL, "NULL plan pointer");
+  *plan = nullptr;
+  std::unique_ptr<mpfft_d_plan> p(new (std::nothrow) mpfft_d_plan);
+  if (!p) return set_err(MPFFT_ENOMEM, "out of host memory");
+  if (int e = d_plan_init_tier(p.get(), n, tier)) return e;
+  *plan = p.release();
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_qd_plan_create(mpfft_d_plan **plan, unsigned long n) {
+  return d_plan_create_tier(plan, n, kTierQD);
+}
+
+MPFFT_API int mpfft_ff_plan_create(mpfft_d_plan **plan, unsigned long n) {
+  return d_plan_create_tier(plan, n, kTierFF);
+}
+
+MPFFT_API int mpfft_multiword_format(const mpfft_d_plan *plan, int *words, int *word_bytes) {
+  if (!plan || !words || !word_bytes) return set_err(MPFFT_EINVAL, "NULL argument");
+  *words = d_words(plan);
+  *word_bytes = (int)d_word_bytes(plan);
+  return set_err(MPFFT_OK, "");
+}
+
+static int multiword_check(const mpfft_d_plan *plan, unsigned long batch) {
+  if (plan->tier < 0) return set_err(MPFFT_EINVAL, "not a double-double, quad-double or float-float plan");
+  if (plan->real || plan->rank > 1) return set_err(MPFFT_EINVAL, "multiword plans are one-dimensional complex plans");
+  if ((unsigned long long)batch * plan->N > (unsigned long long)INT32_MAX)
+    return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  return MPFFT_OK;
+}
+
+MPFFT_API int mpfft_multiword_execute(mpfft_d_plan *plan, unsigned long batch, const void *x, void *y,
+                                      unsigned flags) {
+  if (!plan || !x || !y) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (int e = multiword_check(plan, batch)) return e;
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  std::lock_guard<std::mutex> g(plan->mu);
+  if (int e = d_reserve(plan, batch)) return e;
+  const size_t bytes = (size_t)2 * d_words(plan) * plan->N * batch * d_word_bytes(plan);
+  const bool inv = (flags & MPFFT_INVERSE) != 0;
+  memcpy(plan->h_in, x, bytes);
+  CUDA_TRY(cudaMemcpyAsync(plan->d_in, plan->h_in, bytes, cudaMemcpyHostToDevice, plan->stream));
+  CUDA_TRY(tier_run_transform(plan->tier, plan->tabs, plan->d_in, plan->d_out, (int)batch, d_scale(plan, flags),
+                              plan->stream, inv, inv));
+  CUDA_TRY(cudaMemcpyAsync(plan->h_out, plan->d_out, bytes, cudaMemcpyDeviceToHost, plan->stream));
+  CUDA_TRY(cudaStreamSynchronize(plan->stream));
+  memcpy(y, plan->h_out, bytes);
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_multiword_execute_device(mpfft_d_plan *plan, unsigned long batch, const void *d_in, void *d_out,
+                                             unsigned flags, void *stream) {
+  if (!plan || !d_in || !d_out) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (int e = multiword_check(plan, batch)) return e;
+  if (batch == 0) return set_err(MPFFT_OK, "");
+  const size_t bytes = (size_t)2 * d_words(plan) * plan->N * batch * d_word_bytes(plan);
+  const char *a = (const char *)d_in, *b = (const char *)d_out;
+  if (a < b + bytes && b < a + bytes) return set_err(MPFFT_EINVAL, "input and output buffers overlap");
+  const bool inv = (flags & MPFFT_INVERSE) != 0;
+  CUDA_TRY(tier_run_transform(plan->tier, plan->tabs, d_in, d_out, (int)batch, d_scale(plan, flags),
+                              (cudaStream_t)stream, inv, inv));
   return set_err(MPFFT_OK, "");
 }
 
@@ -1949,7 +2242,7 @@ MPFFT_API int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const dou
                               double *outr, double *outi, unsigned flags) {
   if (!plan || !inr || !ini || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
   if (plan->real) return set_err(MPFFT_EINVAL, "real plan: use mpfft_d_execute_r2c / mpfft_d_execute_c2r");
-  if (plan->dd) return set_err(MPFFT_EINVAL, "double-double plan: use mpfft_dd_execute");
+  if (plan->tier >= 0) return set_err(MPFFT_EINVAL, "multiword plan: use mpfft_multiword_execute (or mpfft_dd_execute)");
   if (batch == 0) return set_err(MPFFT_OK, "");
   if (flags & MPFFT_INVERSE) {  // ifft(X) = swap(FFT(swap(X))) (times 1/n if scaled)
     std::swap(inr, ini);
@@ -1963,19 +2256,23 @@ MPFFT_API int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, co
                                      unsigned flags, void *stream) {
   if (!plan || !d_in || !d_out) return set_err(MPFFT_EINVAL, "NULL argument");
   if (plan->real) return set_err(MPFFT_EINVAL, "real plans have no device-layout entry point");
-  if (plan->dd) return set_err(MPFFT_EINVAL, "double-double plan: use mpfft_dd_execute_device");
+  if (plan->tier >= 0)
+    return set_err(MPFFT_EINVAL, "multiword plan: use mpfft_multiword_execute_device (or mpfft_dd_execute_device)");
   if (batch == 0) return set_err(MPFFT_OK, "");
   const size_t bytes = (size_t)2 * plan->N * batch * 8;
   const char *a = (const char *)d_in, *b = (const char *)d_out;
   if (a < b + bytes && b < a + bytes) return set_err(MPFFT_EINVAL, "input and output buffers overlap");
   if ((unsigned long long)batch * plan->N > (unsigned long long)INT32_MAX)
     return set_err(MPFFT_EUNSUPPORTED, "batch too large");
+  std::lock_guard<std::mutex> g(plan->mu);
   double *tmp = nullptr;
-  {
-    std::lock_guard<std::mutex> g(plan->mu);
-    if (int e = d_tmp_reserve(plan, batch, &tmp)) return e;
-  }
-  CUDA_TRY(d_transform(plan, d_in, d_out, (int)batch, flags, (cudaStream_t)stream, tmp));
+  if (int e = d_tmp_reserve(plan, batch, &tmp)) return e;
+  const cudaStream_t st = (cudaStream_t)stream;
+  if (tmp)
+    if (int e = scratch_wait(plan, st)) return e;
+  CUDA_TRY(d_transform(plan, d_in, d_out, (int)batch, flags, st, tmp));
+  if (tmp)
+    if (int e = scratch_record(plan, st)) return e;
   return set_err(MPFFT_OK, "");
 }
 
@@ -1999,9 +2296,15 @@ MPFFT_API int mpfft_mp_execute_device_timed(mpfft_mp_plan *plan, unsigned long b
   if (plan->host_only) return set_err(MPFFT_EINVAL, "plan was created host-only (conversion only)");
   if (plan->real) return set_err(MPFFT_EINVAL, "real plans have no device-layout entry point");
   if (plan->rank > 1) return set_err(MPFFT_EINVAL, "per-launch timing is for one-dimensional plans");
+  std::lock_guard<std::mutex> g(plan->mu);
   uint32_t *big = nullptr;
   if (int e = mp_big_reserve(plan, batch, &big)) return e;
-  CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, (cudaStream_t)stream, launch_ms, big));
+  const cudaStream_t st = (cudaStream_t)stream;
+  if (big)
+    if (int e = scratch_wait(plan, st)) return e;
+  CUDA_TRY(mp_run_transform(plan->L, plan->tabs, d_in, d_out, (int)batch, st, launch_ms, big));
+  if (big)
+    if (int e = scratch_record(plan, st)) return e;
   return set_err(MPFFT_OK, "");
 }
 
@@ -2014,6 +2317,38 @@ MPFFT_API int mpfft_diag_tc_mul(int limbs, unsigned long batch, const uint32_t *
   if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");
   if (int e = device_ready()) return e;
   CUDA_TRY(mp_tc_mul(limbs, (int)batch, d_x, d_w, d_out, (cudaStream_t)stream));
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_diag_tc_set_wait_limit(unsigned long long ns) {
+  if (int e = device_ready()) return e;
+  CUDA_TRY(mp_tc_set_wait_limit(ns));
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_diag_fail_allocations(long after) {
+  g_alloc_fail_after.store(after < 0 ? -1 : after);
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_mp_plan_counts(const mpfft_mp_plan *plan, unsigned long *mults, unsigned long *adds) {
+  if (!plan || !mults || !adds) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (plan->host_only || plan->rank > 1 || plan->real)
+    return set_err(MPFFT_EINVAL, "op counts are reported for one-dimensional complex device plans");
+  const TreeTables &T = plan->tabs;
+  // leaves: a 4-point DFT is 16 additions, a 2-point one 4 (reference base
+  // cases, lab/parallel/mp/parallel_mp_fft2.c:136-177)
+  unsigned long m = 0, a = 16UL * T.leaf_count[4] + 4UL * T.leaf_count[2];
+  for (int lv = 0; lv < T.nlevels; ++lv) {
+    // per node of size n (q = n/4 butterflies), as the level kernels' step
+    // table runs them: k = 0 no product and 12 additions, k = q/2 four
+    // products and 4 + 12 additions, every other k six products and 6 + 12
+    const unsigned long q = (unsigned long)T.level_n[lv] / 4, cnt = (unsigned long)T.level_count[lv];
+    m += cnt * (4 + 6 * (q - 2));
+    a += cnt * (12 + 16 + 18 * (q - 2));
+  }
+  *mults = m;
+  *adds = a;
   return set_err(MPFFT_OK, "");
 }
 
@@ -2045,6 +2380,13 @@ MPFFT_API int mpfft_mp_execute_significands_static(const mpfft_mp_plan *plan, un
   if (plan->real) return set_err(MPFFT_EINVAL, "real plans have no device-layout entry point");
   if (plan->rank > 1) return set_err(MPFFT_EINVAL, "the static-scratch entry point takes one-dimensional plans");
   if (nl_in < 1 || prec_out < 2) return set_err(MPFFT_EINVAL, "nl_in must be >= 1 and prec_out >= 2");
+  if (flags & ~MPFFT_SCALED) return set_err(MPFFT_EINVAL, "flags 0x%x: only MPFFT_SCALED is accepted here", flags);
+  {
+    int dev = -1;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != plan->device)
+      return set_err(MPFFT_EINVAL, "the current device (%d) is not the plan's device (%d)", dev, plan->device);
+  }
   if (batch == 0) return set_err(MPFFT_OK, "");
   if (batch > (unsigned long)INT32_MAX) return set_err(MPFFT_EUNSUPPORTED, "batch too large");
   if (plan->L > kMaxLimbs || mp_tc_used(plan->tabs, plan->L))
@@ -2052,6 +2394,7 @@ MPFFT_API int mpfft_mp_execute_significands_static(const mpfft_mp_plan *plan, un
                    "the static-scratch entry point supports up to %d limbs on the integer kernels (plan has %d)",
                    kMaxLimbs, plan->L);
   MpPlanView v;
+  v.device = plan->device;
   v.N = plan->N;
   v.L = plan->L;
   v.F = plan->F;

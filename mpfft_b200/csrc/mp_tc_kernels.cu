@@ -59,6 +59,12 @@ constexpr uint32_t kTcTmemCols = 256;
 constexpr uint32_t kTcIdesc = (2u << 4) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 
 __device__ int g_tc_error = 0;  // first error code of any CTA (0 = none)
+// Limit of each wait on this CTA's own MMAs, in ns of %globaltimer.  Only a
+// test changes it (mpfft_diag_tc_set_wait_limit), to make the waits give up.
+__device__ unsigned long long g_tc_wait_ns = 2000000000ull;
+// Limit of the wait that drains a CTA's MMAs before it frees tensor memory
+// after another wait gave up; not affected by the test setting.
+constexpr unsigned long long kTcDrainNs = 2000000000ull;
 
 struct TcGeom {
   int L, Kpad, J0, nt, Q, CL, wzw;
@@ -76,8 +82,8 @@ __host__ __device__ inline TcGeom tc_geom(int L) {
   g.wzw = g.CL / 4 + 8;                   // words of a zero-padded twiddle
   g.offT = 128u * g.Kpad;                 // operand rows first, then 3 x 16 copies
   g.offWZ = g.offT + 48u * g.CL;
-  g.offBar = (g.offWZ + 12u * g.wzw + 15) & ~15u;
-  g.offSlot = g.offBar + 16;
+  g.offBar = (g.offWZ + 12u * g.wzw + 15) & ~15u;  // 3 mbarriers: two buffers, one drain
+  g.offSlot = g.offBar + 32;
   g.bytes = g.offSlot + 16 > kTcMinSmem ? g.offSlot + 16 : kTcMinSmem;
   return g;
 }
@@ -118,10 +124,12 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// wait for the phase with the given parity to complete; false after ~2 s
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// wait for the phase with the given parity to complete; false once `limit` ns
+// have passed (checked before each try, so a limit of 0 gives up at once)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long limit) {
   const uint64_t t0 = global_ns();
   for (;;) {
+    if (global_ns() - t0 >= limit) return false;
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -130,7 +138,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (ok) return true;
-    if (global_ns() - t0 > 2000000000ull) return false;
   }
 }
 
@@ -157,6 +164,7 @@ struct TcCtx {
   uint32_t ph;           // bit b: parity of the next completion of buffer b
   int counter;           // output tiles processed so far (selects the buffer)
   bool bad;              // a wait expired: stop waiting, results are void
+  unsigned long long wait_ns;  // limit of each wait
 };
 
 // all threads; warp 0 allocates the tensor memory
@@ -169,9 +177,11 @@ __device__ void tc_setup(TcCtx &c, uint8_t *smem, int L) {
   c.ph = 0;
   c.counter = 0;
   c.bad = false;
+  c.wait_ns = *(volatile unsigned long long *)&g_tc_wait_ns;
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(c.bar) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(c.bar + 8) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(c.bar + 16) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (threadIdx.x < 32) {
@@ -187,6 +197,19 @@ __device__ void tc_setup(TcCtx &c, uint8_t *smem, int L) {
 }
 
 __device__ void tc_teardown(TcCtx &c, int *err) {
+  // After a wait gave up, MMAs of this CTA may still be writing tensor memory:
+  // thread 0 (which issued them all) commits every MMA it issued to the drain
+  // barrier and waits for it, bounded, before the memory is freed.  A wait
+  // gives up only at the test setting of the limit or after seconds without
+  // progress, so in practice this wait ends within microseconds.
+  if (__syncthreads_or(c.bad ? 1 : 0)) {
+    c.bad = true;
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      tc_commit(c.bar + 16);
+      if (!mbar_wait(c.bar + 16, 0, kTcDrainNs)) atomicCAS(err, 0, 2);  // 2: the drain wait expired too
+    }
+  }
   tc_fence_before();
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -421,7 +444,7 @@ __device__ void tc_product(TcCtx &c, int which, TcEmit &em) {
     const int buf = (c.counter + t) & 1;
     if (threadIdx.x == 0 && t + 1 < G.nt) tc_issue(c, which, t + 1, buf ^ 1);
     __syncwarp();
-    if (!c.bad && !mbar_wait(c.bar + 8u * buf, (c.ph >> buf) & 1u)) c.bad = true;
+    if (!c.bad && !mbar_wait(c.bar + 8u * buf, (c.ph >> buf) & 1u, c.wait_ns)) c.bad = true;
     c.ph ^= 1u << buf;
     tc_fence_after();
     // Tile column n = 8g + r holds output byte column J + g + 16(7 - r), so
@@ -624,6 +647,10 @@ cudaError_t mp_tc_mul(int L, int B, const uint32_t *x, const uint32_t *w, uint32
   if (e != cudaSuccess) return e;
   mp_tc_mul_kernel<<<(B + kTcRows - 1) / kTcRows, kTcRows, G.bytes, s>>>(x, w, out, L, B, err);
   return cudaGetLastError();
+}
+
+cudaError_t mp_tc_set_wait_limit(unsigned long long ns) {
+  return cudaMemcpyToSymbol(g_tc_wait_ns, &ns, sizeof ns);
 }
 
 cudaError_t mp_tc_take_error(int *code) {

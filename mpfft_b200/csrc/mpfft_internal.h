@@ -28,6 +28,7 @@ constexpr int kMaxLevels = 32;
 struct TreeTables {
   int N = 0;
   int nleaves = 0;
+  int leaf_count[5] = {};  // leaves of size 1, 2, 4 (index = size; others unused)
   const Leaf *leaves = nullptr;
   int nlevels = 0;
   int level_n[kMaxLevels] = {};
@@ -72,6 +73,9 @@ struct DDeviceTables {
   const double *wr = nullptr;  // [N/4] cos(2 pi k/N)
   const double *wi = nullptr;  // [N/4] sin(2 pi k/N)
   const double *wrl = nullptr, *wil = nullptr;  // double-double plans: low parts of wr, wi
+  // compensated tiers (float_tier_kernels.cu): the words of cos and sin of
+  // 2 pi k/N, k < N/4 (double-double: 2, quad-double: 4, float-float: 1 double)
+  const double *tw_cos[4] = {}, *tw_sin[4] = {};
   double c8 = 0, c16a = 0, c16b = 0, c16c = 0, c16d = 0;
   // shared-memory sub-transforms (sizes T and T/2) ...
   int nroots = 0;
@@ -84,9 +88,14 @@ struct DDeviceTables {
 constexpr int kMaxDevices = 64;
 constexpr int kDSubMax = 4096;  // FP64: largest shared-memory sub-transform (64 KB)
 constexpr int kDDSubMax = 2048; // double-double: largest shared-memory sub-transform (64 KB)
+constexpr int kQDSubMax = 1024; // quad-double (64 KB)
+constexpr int kFFSubMax = 4096; // float-float (64 KB)
+// compensated floating-point tiers (float_tier_kernels.cu)
+enum { kTierDD = 0, kTierQD = 1, kTierFF = 2 };
 
 // What the static-scratch entry point needs to know about a plan.
 struct MpPlanView {
+  int device = -1;
   unsigned long N = 0;
   int L = 0;
   long F = 0;
@@ -155,6 +164,8 @@ cudaError_t mp_tc_run_levels(int L, const MpDeviceTables &T, uint32_t *out, int 
 cudaError_t mp_tc_mul(int L, int B, const uint32_t *x, const uint32_t *w, uint32_t *out, cudaStream_t s);
 // reads and clears the device-side error flag of the tensor-core kernels
 cudaError_t mp_tc_take_error(int *code);
+// limit of the tensor-core kernels' waits on their own MMAs (ns); tests only
+cudaError_t mp_tc_set_wait_limit(unsigned long long ns);
 size_t mp_tc_smem_bytes(int L);
 inline bool mp_tc_used(const MpDeviceTables &T, int L) {
   return T.tc && L >= (T.tc == 2 ? kTcForceMinLimbs : kTcMinLimbs) && L <= kTcMaxLimbs;
@@ -185,6 +196,13 @@ cudaError_t d_run_transform(const DDeviceTables &T, const double *in, double *ou
 // double-double tier (dd_kernels.cu); layout word (c, h, b, p) at ((c*2 + h)*B + b)*N + p
 cudaError_t dd_run_transform(const DDeviceTables &T, const double *in, double *out, int B, double scale,
                              cudaStream_t s, bool swap_in = false, bool swap_out = false);
+// any compensated tier; layout word (c, h, b, p) at ((c*K + h)*B + b)*N + p with
+// K = tier_words(tier) words of tier_word_bytes(tier) bytes per real component
+cudaError_t tier_run_transform(int tier, const DDeviceTables &T, const void *in, void *out, int B, double scale,
+                               cudaStream_t s, bool swap_in = false, bool swap_out = false);
+int tier_words(int tier);
+size_t tier_word_bytes(int tier);
+int tier_sub_max(int tier);
 // split step of the FP64 real transforms (n = 2M real points), d_kernels.cu
 cudaError_t d_real_split(bool forward, const double *in, double *out, int M, int B, const double *wc,
                          const double *ws, double scale, cudaStream_t s);

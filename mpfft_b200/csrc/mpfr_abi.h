@@ -56,6 +56,8 @@ int mpfr_mul_2si(mpfr_ptr, mpfr_srcptr, long, mpfr_rnd_t);
 int mpfr_add(mpfr_ptr, mpfr_srcptr, mpfr_srcptr, mpfr_rnd_t);
 int mpfr_sub(mpfr_ptr, mpfr_srcptr, mpfr_srcptr, mpfr_rnd_t);
 int mpfr_sub_d(mpfr_ptr, mpfr_srcptr, double, mpfr_rnd_t);
+int mpfr_add_d(mpfr_ptr, mpfr_srcptr, double, mpfr_rnd_t);
+void mpfr_set_prec(mpfr_ptr, mpfr_prec_t);
 double mpfr_get_d(mpfr_srcptr, mpfr_rnd_t);
 int mpfr_abs(mpfr_ptr, mpfr_srcptr, mpfr_rnd_t);
 int mpfr_rint(mpfr_ptr, mpfr_srcptr, mpfr_rnd_t);

@@ -55,18 +55,20 @@ int mp_execute_significands_static(const MpPlanView &v, unsigned long batch, con
                                    const int64_t *d_exp_in, const uint8_t *d_sign_in, int nl_in,
                                    uint64_t *d_mant_out, int64_t *d_exp_out, uint8_t *d_sign_out, long prec_out,
                                    unsigned scaled_shift, cudaStream_t stream, char *msg, size_t msglen) {
-  // scratch layout: input planes | output planes | block exponents
-  const size_t plane_words = (size_t)2 * v.L * v.N * batch;
-  const size_t plane_bytes = (plane_words * 4 + 255) & ~(size_t)255;
-  const size_t need = 2 * plane_bytes + batch * 8;
-  if (need > kStaticScratchBytes) {
-    const size_t per_signal = (size_t)2 * ((size_t)2 * v.L * v.N * 4) + 8;
+  // scratch layout: input planes | output planes | block exponents.  The
+  // bound is a division, so that no product of the caller's sizes can wrap:
+  // each signal takes 2 x (2 L n words) of planes plus an 8-byte exponent,
+  // and the two planes' 256-byte roundings take at most 510 bytes more.
+  const size_t per_signal = (size_t)2 * ((size_t)2 * v.L * v.N * 4) + 8;
+  const size_t max_batch = (kStaticScratchBytes - 512) / per_signal;
+  if (batch > max_batch) {
     snprintf(msg, msglen,
-             "batch %lu of n=%lu needs %zu bytes of scratch; the static scratch holds %zu bytes "
-             "(at most %zu signals at this size)",
-             batch, v.N, need, kStaticScratchBytes, (kStaticScratchBytes - 512) / per_signal);
+             "batch %lu of n=%lu exceeds the static scratch of %zu bytes (at most %zu signals at this size)",
+             batch, v.N, kStaticScratchBytes, max_batch);
     return 2;  // MPFFT_EUNSUPPORTED
   }
+  const size_t plane_words = (size_t)2 * v.L * v.N * batch;
+  const size_t plane_bytes = (plane_words * 4 + 255) & ~(size_t)255;
   void *base = nullptr;
   cudaError_t e = static_scratch_address(&base);
   if (e == cudaSuccess) {

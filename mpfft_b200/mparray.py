@@ -11,6 +11,8 @@ from __future__ import annotations
 
 import ctypes as C
 
+import numpy as np
+
 MPFR_T_SIZE = 32  # sizeof(mpfr_t) on LP64: prec, sign, exp, limb pointer
 _RANDSTATE_SIZE = 64  # >= sizeof(gmp_randstate_t) (32 bytes on LP64)
 
@@ -68,3 +70,17 @@ def fill_uniform(re: MpfrArray, im: MpfrArray, seed: int) -> None:
             _mpfr.mpfr_mul_2ui(p, p, 1, 0)
             _mpfr.mpfr_sub_ui(p, p, 1, 0)
     _gmp.__gmp_randclear(st)
+
+
+def synthetic_planes(n: int, limbs: int, frac_bits: int, batch: int, seed: int = 1) -> np.ndarray:
+    """Limb planes [c][i][p][b] of uniform values in (-1, 1) * 2^F."""
+    rng = np.random.default_rng(seed)
+    words = rng.integers(0, 2**32, size=(2, limbs, n, batch), dtype=np.uint64).astype(np.uint32)
+    top_bits = frac_bits - 32 * (limbs - 1)  # bits of the magnitude in the top limb
+    top = words[:, limbs - 1].astype(np.int64) & ((1 << top_bits) - 1)
+    neg = rng.integers(0, 2, size=top.shape, dtype=np.int64).astype(bool)
+    # two's complement negation of the whole number is not needed for a valid
+    # input: any integer with |A| < 2^F is valid; set the sign by the top limb
+    top = np.where(neg, top - (1 << top_bits), top)
+    words[:, limbs - 1] = (top & 0xFFFFFFFF).astype(np.uint32)
+    return words.reshape(-1)

@@ -51,6 +51,10 @@ OAPI void orc_mp_free(mpfr_t *a, unsigned long n) {
   free(a);
 }
 
+/* a[0] = the number written in s (any MPFR string syntax, e.g. the "%Ra"
+ * hexadecimal form "0x1.8p+3"), rounded to a's precision; 0 on success */
+OAPI int orc_mp_set_str(mpfr_t *a, const char *s) { return mpfr_set_str(a[0], s, 0, RN); }
+
 /* element pointer (lets Python address a[k] of an mpfr_t array) */
 OAPI mpfr_ptr orc_mp_at(mpfr_t *a, unsigned long k) { return a[k]; }
 
@@ -404,6 +408,98 @@ OAPI void orc_mp_fft(orc_mp_ctx *c, unsigned long n, unsigned long s, long sn,
 /* Top-level convenience: full forward transform of n = N contiguous points. */
 OAPI void orc_mp_fft_top(orc_mp_ctx *c, mpfr_t *xr, mpfr_t *xi, mpfr_t *yr, mpfr_t *yi) {
   orc_mp_fft(c, c->N, 1, 0, xr, xi, yr, yi);
+}
+
+/* ------------------------------------------------------------------------ */
+/* the weighted power loss of the adjoint configuration                     */
+/* ------------------------------------------------------------------------ */
+
+/* Multiword views (the compensated tiers' formats): out[h*stride + k] = word
+ * h of a[k], h < K -- the nearest double (or float, is_float) to a[k], then
+ * the nearest to what is left, ...  set: a[k] = the words' exact sum rounded
+ * to a's precision. */
+OAPI void orc_mp_get_words(mpfr_t *a, unsigned long n, int K, int is_float, void *out, unsigned long stride) {
+  mpfr_t t;
+  mpfr_init2(t, 64);
+  for (unsigned long k = 0; k < n; k++) {
+    if (mpfr_get_prec(t) < mpfr_get_prec(a[k])) mpfr_set_prec(t, mpfr_get_prec(a[k]));
+    mpfr_set(t, a[k], RN);
+    for (int h = 0; h < K; h++) {
+      double w = mpfr_get_d(t, RN);
+      if (is_float) w = (double)(float)w;
+      mpfr_sub_d(t, t, w, RN);
+      if (is_float) ((float *)out)[h * stride + k] = (float)w;
+      else ((double *)out)[h * stride + k] = w;
+    }
+  }
+  mpfr_clear(t);
+}
+
+OAPI void orc_mp_set_words(mpfr_t *a, unsigned long n, int K, int is_float, const void *in, unsigned long stride) {
+  mpfr_t acc;
+  mpfr_init2(acc, 2200);
+  for (unsigned long k = 0; k < n; k++) {
+    mpfr_set_ui(acc, 0, RN);
+    for (int h = 0; h < K; h++)
+      mpfr_add_d(acc, acc, is_float ? (double)((const float *)in)[h * stride + k] : ((const double *)in)[h * stride + k],
+                 RN);
+    mpfr_set(a[k], acc, RN);
+  }
+  mpfr_clear(acc);
+}
+
+/* a[0] -= b[0] (rounded to a's precision) */
+OAPI void orc_mp_sub_into(mpfr_t *a, mpfr_t *b) { mpfr_sub(a[0], a[0], b[0], RN); }
+
+/* a[k] *= w[k] (rounded to a's precision) */
+OAPI void orc_mp_mul_d(mpfr_t *a, const double *w, unsigned long n) {
+  for (unsigned long k = 0; k < n; k++) mpfr_mul_d(a[k], a[k], w[k], RN);
+}
+
+/* out[0] = L(x) = sum_k w_k |X_k|^2 with X = the reference transform of x at
+ * the context's precision (summed at out's precision) */
+OAPI void orc_mp_power_loss(orc_mp_ctx *c, const double *w, mpfr_t *xr, mpfr_t *xi, mpfr_t *out) {
+  const unsigned long n = c->N;
+  mpfr_t *yr = orc_mp_alloc(n, c->P), *yi = orc_mp_alloc(n, c->P);
+  orc_mp_fft(c, n, 1, 0, xr, xi, yr, yi);
+  mpfr_t t, u;
+  mpfr_inits2(mpfr_get_prec(out[0]), t, u, (mpfr_ptr)0);
+  mpfr_set_ui(out[0], 0, RN);
+  for (unsigned long k = 0; k < n; k++) {
+    mpfr_mul(t, yr[k], yr[k], RN);
+    mpfr_mul(u, yi[k], yi[k], RN);
+    mpfr_add(t, t, u, RN);
+    mpfr_mul_d(t, t, w[k], RN);
+    mpfr_add(out[0], out[0], t, RN);
+  }
+  mpfr_clears(t, u, (mpfr_ptr)0);
+  orc_mp_free(yr, n);
+  orc_mp_free(yi, n);
+}
+
+/* Central difference of the loss above in component j (part 0 real, 1
+ * imaginary) with step h = 2^h_exp:  out[0] = (L(x + h e) - L(x - h e)) / 2h.
+ * L is quadratic in x, so the central difference has no truncation error:
+ * out equals dL/dx_j up to the rounding of the two losses.  x is restored. */
+OAPI void orc_mp_power_loss_fd(orc_mp_ctx *c, const double *w, mpfr_t *xr, mpfr_t *xi, unsigned long j, int part,
+                               long h_exp, mpfr_t *out) {
+  mpfr_ptr xj = part ? xi[j] : xr[j];
+  const long pw = mpfr_get_prec(out[0]);
+  mpfr_t save, lp, lm;
+  mpfr_init2(save, mpfr_get_prec(xj));
+  mpfr_inits2(pw, lp, lm, (mpfr_ptr)0);
+  mpfr_set(save, xj, RN);
+  mpfr_t h;
+  mpfr_init2(h, 2);
+  mpfr_set_ui_2exp(h, 1, h_exp, RN);
+  mpfr_add(xj, save, h, RN);
+  orc_mp_power_loss(c, w, xr, xi, &lp);
+  mpfr_sub(xj, save, h, RN);
+  orc_mp_power_loss(c, w, xr, xi, &lm);
+  mpfr_set(xj, save, RN);
+  mpfr_sub(out[0], lp, lm, RN);
+  mpfr_div_2si(out[0], out[0], h_exp + 1, RN);
+  mpfr_clears(save, lp, lm, h, (mpfr_ptr)0);
 }
 
 /* ------------------------------------------------------------------------ */

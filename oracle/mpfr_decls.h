@@ -131,6 +131,8 @@ int mpfr_mul_ui(mpfr_ptr, mpfr_srcptr, unsigned long, mpfr_rnd_t);
 int mpfr_div_ui(mpfr_ptr, mpfr_srcptr, unsigned long, mpfr_rnd_t);
 int mpfr_ui_div(mpfr_ptr, unsigned long, mpfr_srcptr, mpfr_rnd_t);
 int mpfr_mul_2si(mpfr_ptr, mpfr_srcptr, long, mpfr_rnd_t);
+int mpfr_div_2si(mpfr_ptr, mpfr_srcptr, long, mpfr_rnd_t);
+int mpfr_mul_d(mpfr_ptr, mpfr_srcptr, double, mpfr_rnd_t);
 int mpfr_mul_2ui(mpfr_ptr, mpfr_srcptr, unsigned long, mpfr_rnd_t);
 int mpfr_div_2ui(mpfr_ptr, mpfr_srcptr, unsigned long, mpfr_rnd_t);
 int mpfr_log2(mpfr_ptr, mpfr_srcptr, mpfr_rnd_t);

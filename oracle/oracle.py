@@ -47,6 +47,7 @@ def lib() -> C.CDLL:
         "orc_mp_alloc": (vp, [ul, sl]),
         "orc_mp_free": (None, [vp, ul]),
         "orc_mp_at": (vp, [vp, ul]),
+        "orc_mp_set_str": (C.c_int, [vp, C.c_char_p]),
         "orc_mp_copy": (None, [vp, vp, ul]),
         "orc_mp_gather": (None, [vp, vp, ul, ul]),
         "orc_mp_set_prec_all": (None, [vp, ul, sl]),
@@ -68,6 +69,12 @@ def lib() -> C.CDLL:
         "orc_mp_fft": (None, [vp, ul, ul, sl, vp, vp, vp, vp]),
         "orc_mp_fft_top": (None, [vp, vp, vp, vp, vp]),
         "orc_mp_dft": (None, [ul, sl, vp, vp, vp, vp]),
+        "orc_mp_mul_d": (None, [vp, vp, ul]),
+        "orc_mp_sub_into": (None, [vp, vp]),
+        "orc_mp_get_words": (None, [vp, ul, C.c_int, C.c_int, vp, ul]),
+        "orc_mp_set_words": (None, [vp, ul, C.c_int, C.c_int, vp, ul]),
+        "orc_mp_power_loss": (None, [vp, vp, vp, vp, vp]),
+        "orc_mp_power_loss_fd": (None, [vp, vp, vp, vp, ul, C.c_int, sl, vp]),
         "orc_mp_hermitian_extend": (None, [ul, vp, vp, vp, vp]),
         "orc_mp_dft_nd": (None, [C.c_int, C.POINTER(C.c_ulong), sl, vp, vp, vp, vp]),
         "orc_mp_get_dd": (None, [vp, vp, vp, ul]),

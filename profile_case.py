@@ -2,7 +2,7 @@
 
 A small, self-contained driver for profilers (ncu) and quick timing:
 
-    python -m mpfft_b200.profile_case --n 1024 --prec 1024 --batch 512 --reps 2
+    python profile_case.py --n 1024 --prec 1024 --batch 512 --reps 2
 
 The input planes are random two's-complement fixed-point values of magnitude
 below 2^F (F = the plan's fraction bits), i.e. a block-normalised signal with
@@ -12,22 +12,13 @@ produces.  Prints per-launch milliseconds of the last repetition.
 from __future__ import annotations
 
 import argparse
+import os
+import sys
 
 import numpy as np
 
-
-def synthetic_planes(n: int, limbs: int, frac_bits: int, batch: int, seed: int = 1) -> np.ndarray:
-    """Limb planes [c][i][p][b] of uniform values in (-1, 1) * 2^F."""
-    rng = np.random.default_rng(seed)
-    words = rng.integers(0, 2**32, size=(2, limbs, n, batch), dtype=np.uint64).astype(np.uint32)
-    top_bits = frac_bits - 32 * (limbs - 1)  # bits of the magnitude in the top limb
-    top = words[:, limbs - 1].astype(np.int64) & ((1 << top_bits) - 1)
-    neg = rng.integers(0, 2, size=top.shape, dtype=np.int64).astype(bool)
-    # two's complement negation of the whole number is not needed for a valid
-    # input: any integer with |A| < 2^F is valid; set the sign by the top limb
-    top = np.where(neg, top - (1 << top_bits), top)
-    words[:, limbs - 1] = (top & 0xFFFFFFFF).astype(np.uint32)
-    return words.reshape(-1)
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from mpfft_b200.mparray import synthetic_planes  # noqa: E402
 
 
 def run_fp64(a) -> None:

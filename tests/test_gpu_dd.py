@@ -96,3 +96,58 @@ def test_dd_batch_scaled_inverse_device(M, orc):
             ref = (hr, hi_)
         assert np.array_equal(out[0], ref[0][0]) and np.array_equal(out[1], ref[0][1])
         assert np.array_equal(out[2], ref[1][0]) and np.array_equal(out[3], ref[1][1])
+
+
+def _ref212_error(O, xr_pair, xi_pair, yr_pair, yi_pair, n):
+    """log2 normwise error of a double-double output against the reference's
+    transform run at 212 bits on the same (exactly converted) input."""
+    xr, xi = _to_mp(O, xr_pair, 212), _to_mp(O, xi_pair, 212)
+    gr, gi = _to_mp(O, yr_pair, 212), _to_mp(O, yi_pair, 212)
+    wr, wi = O.mp_pair(n, 212)
+    O.MpFFT(n, 212)(xr, xi, wr, wi)
+    return O.mp_errors(gr, gi, wr, wi)["log2_rel"]
+
+
+@pytest.mark.parametrize("lg", [15, 16, 17, 18, 19, 20])
+def test_dd_single_signal_large_n_vs_reference_212(M, orc, lg):
+    """Single signals N = 2^15 .. 2^20 (above the direct DFT's reach) against
+    the reference transform at 212 bits (lab/serial/mp/serial_mp_fft3.c,
+    restated bit for bit by the oracle)."""
+    O = orc
+    n = 1 << lg
+    _, _, pr, pi = _dd_inputs(O, n, 1, 500 + lg)
+    plan = M.DDPlan(n)
+    yr = (np.zeros(n), np.zeros(n))
+    yi = (np.zeros(n), np.zeros(n))
+    plan.execute(1, pr, pi, yr, yi)
+    e = _ref212_error(O, pr, pi, yr, yi, n)
+    assert e <= np.log2(8 * lg) - 104, (n, e)
+
+
+def test_dd_batch_4096_signals_of_4096(M, orc):
+    """The batched configuration: 4096 signals of N=4096 in one call; sampled
+    signals (both ends and the middle of the batch) against the reference at
+    212 bits, and bit-equal to single-signal calls."""
+    O = orc
+    n, batch = 4096, 4096
+    rng = np.random.default_rng(20261203)
+    parts = []
+    for _ in range(2):  # double-double inputs hi + lo with |lo| < ulp(hi)/2
+        hi = rng.uniform(-1, 1, n * batch)
+        parts.append((hi, hi * rng.uniform(-1, 1, n * batch) * 2.0 ** -54))
+    pr, pi = parts
+    plan = M.DDPlan(n)
+    z = lambda: (np.zeros(n * batch), np.zeros(n * batch))
+    yr, yi = z(), z()
+    plan.execute(batch, pr, pi, yr, yi)
+    for b in (0, 1, 2047, 2048, 4094, 4095):
+        s = slice(b * n, (b + 1) * n)
+        cut = lambda pair: (np.ascontiguousarray(pair[0][s]), np.ascontiguousarray(pair[1][s]))
+        e = _ref212_error(O, cut(pr), cut(pi), cut(yr), cut(yi), n)
+        assert e <= np.log2(8 * 12) - 104, (b, e)
+    for b in (0, batch - 1):
+        s = slice(b * n, (b + 1) * n)
+        sr, si = (np.zeros(n), np.zeros(n)), (np.zeros(n), np.zeros(n))
+        plan.execute(1, (pr[0][s].copy(), pr[1][s].copy()), (pi[0][s].copy(), pi[1][s].copy()), sr, si)
+        for got, ref in ((sr, yr), (si, yi)):
+            assert np.array_equal(got[0], ref[0][s]) and np.array_equal(got[1], ref[1][s])

@@ -124,7 +124,7 @@ def test_mp_small_batch_level_kernel_bit_identical(M, p):
     give bit-identical outputs."""
     import torch
 
-    from mpfft_b200.profile_case import synthetic_planes
+    from mpfft_b200.mparray import synthetic_planes
 
     n, B = 1024, 2048
     plan = M.MpPlan(n, p)

@@ -65,8 +65,23 @@ def test_static_scratch_entry_matches_allocating_entry(orc):
         assert L.orc_mp_count_diff(yr.ptr, zr.ptr, n * batch) == 0, f"call {call}"
         assert L.orc_mp_count_diff(yi.ptr, zi.ptr, n * batch) == 0, f"call {call}"
 
-    # a batch beyond the static array is rejected before any device work
+        if call == 1:
+            # the defining property: a further call changes the device's free
+            # memory by nothing (no allocation of any kind, cached or not)
+            free0 = torch.cuda.mem_get_info()[0]
+            plan.execute_significands_static(batch, d_m.data_ptr(), d_e.data_ptr(), d_s.data_ptr(), nl,
+                                             o_m.data_ptr(), o_e.data_ptr(), o_s.data_ptr(), prec, scaled=scaled,
+                                             stream=stream.cuda_stream)
+            torch.cuda.synchronize()
+            assert torch.cuda.mem_get_info()[0] == free0
+
+    # a batch beyond the static array is rejected before any device work, also
+    # where the caller's sizes would wrap a product of them
     too_big = M.lib.mpfft_static_scratch_bytes() // (16 * plan.limbs * n) + 1
-    with pytest.raises(M.MpfftError) as e:
-        plan.execute_significands_static(too_big, 1, 1, 1, nl, 1, 1, 1, prec)
-    assert e.value.code == M.EUNSUPPORTED
+    for bad in (too_big, 2**62):
+        with pytest.raises(M.MpfftError) as e:
+            plan.execute_significands_static(bad, 1, 1, 1, nl, 1, 1, 1, prec)
+        assert e.value.code in (M.EUNSUPPORTED,)
+    # only MPFFT_SCALED is accepted: an inverse request is an error, not a forward transform
+    rc = M.lib.mpfft_mp_execute_significands_static(plan.h, 1, 1, 1, 1, nl, 1, 1, 1, prec, M.INVERSE, None)
+    assert rc == M.EINVAL
