@@ -65,6 +65,9 @@ extern "C" {
 #define MPFFT_PLAN_TENSOR 32u    /* plan creation: tensor-core twiddle products from 8 limbs up */
 #define MPFFT_PLAN_FLOAT_TIERS 64u /* plan creation: run host-array transforms of precisions up to 200 bits on a
                                        compensated floating-point tier (see mpfft_mp_plan_form) */
+#define MPFFT_PLAN_NATIVE_TIERS 128u /* plan creation: precisions up to 212 bits on the smallest floating word format
+                                         holding P bits (float-float 48, FP64 53, double-double 106,
+                                         quad-double 212), with that tier's own error */
 
 /* the form an mp plan's host-array transforms run in (mpfft_mp_plan_form) */
 #define MPFFT_FORM_LIMBS 0         /* fixed-point 32-bit limbs, integer pipes */
@@ -290,6 +293,60 @@ int mpfft_d_execute(mpfft_d_plan *plan, unsigned long batch, const double *inr, 
 int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, const double *d_in, double *d_out,
                            unsigned flags, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* uneven batches in one graph launch (no counterpart in the reference,      */
+/* which transforms one signal per call and parallelises one butterfly loop  */
+/* with an OpenMP team per node, lab/parallel/mp/parallel_mp_fft2.c:259-326) */
+/* ------------------------------------------------------------------------ */
+
+/* A batch plan for `count` signals of lengths n[i] (powers of two, up to 2^22)
+ * and precisions prec[i] bits.  Each signal gets a form: fixed-point limbs
+ * (up to 34 limbs), or with MPFFT_PLAN_FLOAT_TIERS / MPFFT_PLAN_NATIVE_TIERS the
+ * floating tier mpfft_mp_plan_form names for that precision.  Signals are grouped into
+ * one queue per form (per limb count for limbs); each queue is a persistent
+ * kernel whose CTAs take whole signals, largest first, from a device counter
+ * and transform them end to end, and the whole batch is captured as one CUDA
+ * graph (created here, replayed by every execute).  Every output is
+ * bit-identical to a single call of the same signal through
+ * mpfft_mp_plan_create_flags with the same flags.  The plan owns an input and
+ * an output arena in device memory holding every signal in its form's layout
+ * (mpfft_batch_signal_format).  Choices made by mpfft_batch_autotune for the
+ * same kind of batch on the same device are read back from the tune file. */
+typedef struct mpfft_batch_plan mpfft_batch_plan;
+int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long count, const unsigned long *n, const long *prec,
+                            unsigned flags);
+int mpfft_batch_plan_destroy(mpfft_batch_plan *plan);
+/* Form of signal i (MPFFT_FORM_*), its words per real component (the limb
+ * count for MPFFT_FORM_LIMBS: limb planes [c][i][p] of 32-bit words, else the
+ * tier's K: words [c][h][p], doubles or, for float-float, floats), and its byte
+ * offset and size in the arenas. */
+int mpfft_batch_signal_format(const mpfft_batch_plan *plan, unsigned long i, int *form, int *words, size_t *offset,
+                              size_t *bytes);
+/* device addresses and size of the input and output arenas */
+int mpfft_batch_arenas(const mpfft_batch_plan *plan, void **d_in, void **d_out, size_t *bytes);
+/* One graph launch on `stream`: every signal of the input arena into the
+ * output arena (forward, unscaled).  Asynchronous. */
+int mpfft_batch_execute_device(mpfft_batch_plan *plan, void *stream);
+/* Host mpfr_t arrays, signal i at inr[i][0..n[i]) etc.: converted into the
+ * arena on the host (limb signals with one block exponent each, floating
+ * signals split into words), one copy each way, one graph launch.  flags:
+ * MPFFT_SCALED, MPFFT_INVERSE.  A floating signal with exponents outside its
+ * tier's window is rejected with MPFFT_EUNSUPPORTED.  Synchronous. */
+int mpfft_batch_execute(mpfft_batch_plan *plan, mpfr_t *const *inr, mpfr_t *const *ini, mpfr_t *const *outr,
+                        mpfr_t *const *outi, unsigned flags);
+/* The autotuner: per queue, times every candidate launch shape -- CTA size
+ * and, for floating forms, the largest shared-memory sub-transform -- on the
+ * plan's own signals (the input arena as it is), keeps the fastest, re-captures
+ * the graph and, when save != 0, records the choices in the tune file
+ * (MPFFT_AUTOTUNE_FILE, else $XDG_CACHE_HOME/mpfft_b200/autotune.json, else
+ * ~/.cache/mpfft_b200/autotune.json).  No choice changes any result. */
+int mpfft_batch_autotune(mpfft_batch_plan *plan, int save);
+/* Queue q of the plan: family (0 limbs, 1 FP64, 2 double-double,
+ * 3 quad-double, 4 float-float), limb count, CTA size, largest sub-transform,
+ * signal count.  q < 0: returns the number of queues. */
+int mpfft_batch_queue_info(const mpfft_batch_plan *plan, int q, int *family, int *limbs, int *threads, int *sub,
+                           int *signals);
+
 /* Transform `batch` signals whose MPFR fields are already in device memory,
  * WITHOUT allocating anything: no cudaMalloc, cudaFree or other allocating
  * call.  No counterpart in the reference.  For callers that cannot allocate
@@ -337,6 +394,10 @@ int mpfft_mp_execute_device_timed(mpfft_mp_plan *plan, unsigned long batch, cons
 /* Measured integer multiply-add rate of the current GPU (ops/s): wide = 0 for
  * 32-bit multiply-add, 1 for 32x32+64 -> 64-bit multiply-add. */
 int mpfft_diag_imad_rate(int wide, double *ops_per_s);
+/* Measured int8 tensor-core rate of the current GPU: unsigned-byte
+ * multiply-adds per second of back-to-back tcgen05.mma kind::i8 (M=128,
+ * N=256, K=32) from shared memory into tensor memory, two CTAs per SM. */
+int mpfft_diag_tc_int8_rate(double *macs_per_s);
 /* The tensor-core twiddle product on its own: out = sign(x) * r for `batch`
  * operands x (device limb planes x[i*batch + b], two's complement, L limbs,
  * |x| < 2^(32L-2)) and one unsigned twiddle w[0..L-1], with

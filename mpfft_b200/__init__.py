@@ -31,6 +31,7 @@ INVERSE = 8
 PLAN_NO_TENSOR = 16
 PLAN_TENSOR = 32
 PLAN_FLOAT_TIERS = 64
+PLAN_NATIVE_TIERS = 128
 FORM_LIMBS, FORM_TENSOR, FORM_FLOAT_FLOAT, FORM_DOUBLE, FORM_DOUBLE_DOUBLE, FORM_QUAD_DOUBLE = range(6)
 
 
@@ -102,11 +103,22 @@ def _load() -> C.CDLL:
         "mpfft_diag_fail_allocations": (C.c_int, [C.c_long]),
         "mpfft_mp_plan_counts": (C.c_int, [vp, C.POINTER(C.c_ulong), C.POINTER(C.c_ulong)]),
         "mpfft_mp_plan_form": (C.c_int, [vp]),
+        "mpfft_diag_tc_int8_rate": (C.c_int, [C.POINTER(C.c_double)]),
         "mpfft_qd_plan_create": (C.c_int, [C.POINTER(vp), ul]),
         "mpfft_ff_plan_create": (C.c_int, [C.POINTER(vp), ul]),
         "mpfft_multiword_format": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "mpfft_multiword_execute": (C.c_int, [vp, ul, vp, vp, C.c_uint]),
         "mpfft_multiword_execute_device": (C.c_int, [vp, ul, vp, vp, C.c_uint, vp]),
+        "mpfft_batch_plan_create": (C.c_int, [C.POINTER(vp), ul, C.POINTER(ul), C.POINTER(sl), C.c_uint]),
+        "mpfft_batch_plan_destroy": (C.c_int, [vp]),
+        "mpfft_batch_signal_format": (C.c_int, [vp, ul, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                                C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+        "mpfft_batch_arenas": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(C.c_size_t)]),
+        "mpfft_batch_execute_device": (C.c_int, [vp, vp]),
+        "mpfft_batch_execute": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_uint]),
+        "mpfft_batch_autotune": (C.c_int, [vp, C.c_int]),
+        "mpfft_batch_queue_info": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                             C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -190,14 +202,16 @@ class MpPlan:
     """Multiprecision plan for n points at `prec` bits (device limb format)."""
 
     def __init__(self, n: int, prec: int, host_only: bool = False, host_conversion: bool = False,
-                 tensor=True, float_tiers: bool = False):
+                 tensor=True, float_tiers=False):
         """tensor: True (default choice), False (integer pipes only) or
-        "force" (tensor-core products from 8 limbs up).  float_tiers: run
-        precisions a compensated floating-point tier covers on that tier."""
+        "force" (tensor-core products from 8 limbs up).  float_tiers: True runs
+        precisions a compensated floating-point tier covers within the mp
+        error contract on that tier; "native" picks the smallest word format
+        holding P bits."""
         h = C.c_void_p()
         flags = ((PLAN_HOST_ONLY if host_only else 0) | (PLAN_HOST_CONVERSION if host_conversion else 0)
                  | (PLAN_TENSOR if tensor == "force" else 0 if tensor else PLAN_NO_TENSOR)
-                 | (PLAN_FLOAT_TIERS if float_tiers else 0))
+                 | (PLAN_NATIVE_TIERS if float_tiers == "native" else PLAN_FLOAT_TIERS if float_tiers else 0))
         _check(lib.mpfft_mp_plan_create_flags(C.byref(h), n, prec, flags))
         self.h = h
         self.n, self.prec = n, prec
@@ -334,6 +348,13 @@ def fail_allocations(after: int) -> None:
     _check(lib.mpfft_diag_fail_allocations(after))
 
 
+def tc_int8_rate() -> float:
+    """Measured int8 tensor-core multiply-add rate of the current GPU, MAC/s."""
+    v = C.c_double()
+    _check(lib.mpfft_diag_tc_int8_rate(C.byref(v)))
+    return v.value
+
+
 def imad_rate(wide: bool = False) -> float:
     """Measured integer multiply-add rate of the current GPU, ops/s."""
     v = C.c_double()
@@ -438,3 +459,56 @@ class MultiwordPlan(DPlan):
     def execute_device(self, batch, d_in: int, d_out: int, scaled=False, stream: int = 0, inverse=False) -> None:
         flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
         _check(lib.mpfft_multiword_execute_device(self.h, batch, d_in, d_out, flags, stream or None))
+
+
+class BatchPlan:
+    """Uneven batch (lengths ns, precisions precs) as one graph launch of the
+    persistent work-queue kernels; float_tiers as for MpPlan."""
+
+    def __init__(self, ns, precs, float_tiers=False):
+        k = len(ns)
+        h = C.c_void_p()
+        _check(lib.mpfft_batch_plan_create(C.byref(h), k, (C.c_ulong * k)(*ns), (C.c_long * k)(*precs),
+                                           PLAN_NATIVE_TIERS if float_tiers == "native"
+                                           else PLAN_FLOAT_TIERS if float_tiers else 0))
+        self.h = h
+        self.count = k
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.mpfft_batch_plan_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def signal_format(self, i: int) -> tuple[int, int, int, int]:
+        """(form, words or limbs, byte offset, bytes) of signal i in the arenas."""
+        f, w, o, b = C.c_int(), C.c_int(), C.c_size_t(), C.c_size_t()
+        _check(lib.mpfft_batch_signal_format(self.h, i, C.byref(f), C.byref(w), C.byref(o), C.byref(b)))
+        return f.value, w.value, o.value, b.value
+
+    def arenas(self) -> tuple[int, int, int]:
+        a, b, n = C.c_void_p(), C.c_void_p(), C.c_size_t()
+        _check(lib.mpfft_batch_arenas(self.h, C.byref(a), C.byref(b), C.byref(n)))
+        return a.value, b.value, n.value
+
+    def execute_device(self, stream: int = 0) -> None:
+        _check(lib.mpfft_batch_execute_device(self.h, stream or None))
+
+    def execute(self, inr, ini, outr, outi, scaled=False, inverse=False) -> None:
+        arr = lambda v: (C.c_void_p * self.count)(*v)
+        flags = (SCALED if scaled else 0) | (INVERSE if inverse else 0)
+        _check(lib.mpfft_batch_execute(self.h, arr(inr), arr(ini), arr(outr), arr(outi), flags))
+
+    def autotune(self, save: bool = True) -> None:
+        _check(lib.mpfft_batch_autotune(self.h, 1 if save else 0))
+
+    def queues(self) -> list[dict]:
+        z = C.c_int()
+        nq = lib.mpfft_batch_queue_info(self.h, -1, C.byref(z), C.byref(z), C.byref(z), C.byref(z), C.byref(z))
+        out = []
+        for q in range(nq):
+            v = [C.c_int() for _ in range(5)]
+            _check(lib.mpfft_batch_queue_info(self.h, q, *[C.byref(x) for x in v]))
+            out.append(dict(zip(("family", "limbs", "threads", "sub", "signals"), [x.value for x in v])))
+        return out

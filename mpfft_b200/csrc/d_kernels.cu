@@ -20,221 +20,11 @@
 #include <algorithm>
 #include <cstdint>
 
+#include "d_core.cuh"
 #include "mpfft_internal.h"
 
 namespace mpfft {
 
-struct DConst {
-  double c8, c16a, c16b, c16c, c16d;
-};
-
-// 8-point base case on one part (reference :153-191); v = b1..b8
-__device__ __forceinline__ void d8_part(const DConst &K, const double *x, double *v) {
-  const double s04 = x[0] + x[4], d04 = x[0] - x[4];
-  const double s26 = x[2] + x[6], d26 = x[2] - x[6];
-  const double s17 = x[1] + x[7], d17 = x[1] - x[7];
-  const double s35 = x[3] + x[5], d35 = x[3] - x[5];
-  const double p = K.c8 * (d17 + d35);
-  const double q = K.c8 * (s17 - s35);
-  v[0] = s17 + s35;
-  v[1] = s04 + s26;
-  v[2] = s04 - s26;
-  v[3] = d17 - d35;
-  v[4] = d04 + q;
-  v[5] = d04 - q;
-  v[6] = d26 + p;
-  v[7] = d26 - p;
-}
-
-struct D16 {
-  double b5, b6, b11, b12, c1, c2, c3, c4, c9, c10, c11, c12, c17, c18, c19, c20;
-};
-
-// 16-point base case on one part (reference :218-348); the imaginary-part
-// variant has a10, b3, b12 and the products m2, m4, m5, m6, m7 with the
-// opposite sign convention, exactly as the reference writes them.
-__device__ __forceinline__ void d16_part(const DConst &K, const double *x, bool im, D16 &o) {
-  double s[8], d[8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    s[j] = x[j] + x[j + 8];
-    d[j] = x[j] - x[j + 8];
-  }
-  const double a10 = im ? (-x[4] + x[12]) : d[4];
-  const double b1 = s[0] - s[4], b2 = s[0] + s[4];
-  const double b3 = im ? (-s[2] + s[6]) : (s[2] - s[6]);
-  const double b4 = s[2] + s[6];
-  const double b7 = s[1] - s[5], b8 = s[1] + s[5];
-  const double b9 = s[3] - s[7], b10 = s[3] + s[7];
-  const double b13 = d[1] + d[7], b14 = d[1] - d[7];
-  const double b15 = d[3] + d[5], b16 = d[5] - d[3];
-  o.b5 = b2 + b4;
-  o.b6 = b2 - b4;
-  o.b11 = b8 + b10;
-  o.b12 = im ? (-b8 + b10) : (b8 - b10);
-  const double m1 = K.c8 * (d[2] - d[6]);
-  const double m2 = (im ? -K.c8 : K.c8) * (d[2] + d[6]);
-  const double m3 = K.c8 * (b7 - b9);
-  const double m4 = (im ? -K.c8 : K.c8) * (b7 + b9);
-  const double m5 = (im ? -K.c16a : K.c16a) * (b13 + b15);
-  const double m6 = (im ? K.c16b : -K.c16b) * b13;
-  const double m7 = (im ? -K.c16d : K.c16d) * b15;
-  const double m8 = K.c16c * (b14 + b16);
-  const double m9 = K.c16d * b14;
-  const double m10 = -K.c16b * b16;
-  o.c1 = b1 + m3;
-  o.c2 = b1 - m3;
-  o.c3 = b3 + m4;
-  o.c4 = m4 - b3;
-  const double c5 = d[0] + m1, c6 = d[0] - m1;
-  const double c7 = m9 - m8, c8 = m10 - m8;
-  o.c9 = c5 + c7;
-  o.c10 = c5 - c7;
-  o.c11 = c6 + c8;
-  o.c12 = c6 - c8;
-  const double c13 = a10 + m2, c14 = a10 - m2;
-  const double c15 = m5 + m6, c16 = m5 - m7;
-  o.c17 = c13 + c15;
-  o.c18 = c13 - c15;
-  o.c19 = c14 + c16;
-  o.c20 = c14 - c16;
-}
-
-// Shared-memory index: the low 4 bits of m XOR-ed with bits 4-7 ^ 8-11 (a
-// permutation inside every 16-aligned block, so a plane needs no padding).
-// Leaves work on 16 (or 8) consecutive elements per thread, levels on
-// consecutive k, the DIT gather on scattered positions; over the whole
-// 4096-point schedule this needs 29 % fewer shared-memory wavefronts than one
-// pad slot per 16 elements (counted by simulating every access of the
-// schedule per half-warp and bank).
-__device__ __forceinline__ int pidx(int m) { return m ^ (((m >> 4) ^ (m >> 8)) & 15); }
-
-// Leaf of size 16 at positions [o, o+16) (reference :213-385), in place.
-__device__ __forceinline__ void d_leaf16(const DConst &K, double *yr, double *yi, int o) {
-  double xr[16], xi[16];
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    xr[j] = yr[pidx(o + j)];
-    xi[j] = yi[pidx(o + j)];
-  }
-  D16 R, I;
-  d16_part(K, xr, false, R);
-  d16_part(K, xi, true, I);
-  // output stage (reference :350-382)
-  double *r = yr, *i = yi;
-#define P(j) pidx(o + (j))
-  r[P(0)] = R.b5 + R.b11;  r[P(8)] = R.b5 - R.b11;
-  i[P(0)] = I.b5 + I.b11;  i[P(8)] = I.b5 - I.b11;
-  r[P(4)] = R.b6 - I.b12;  r[P(12)] = R.b6 + I.b12;
-  i[P(4)] = I.b6 - R.b12;  i[P(12)] = I.b6 + R.b12;
-  r[P(1)] = R.c9 - I.c17;  r[P(15)] = R.c9 + I.c17;
-  i[P(1)] = I.c9 - R.c17;  i[P(15)] = I.c9 + R.c17;
-  r[P(2)] = R.c1 - I.c3;   r[P(14)] = R.c1 + I.c3;
-  i[P(2)] = I.c1 - R.c3;   i[P(14)] = I.c1 + R.c3;
-  r[P(3)] = R.c12 + I.c20; r[P(13)] = R.c12 - I.c20;
-  i[P(3)] = I.c12 + R.c20; i[P(13)] = I.c12 - R.c20;
-  r[P(5)] = R.c11 - I.c19; r[P(11)] = R.c11 + I.c19;
-  i[P(5)] = I.c11 - R.c19; i[P(11)] = I.c11 + R.c19;
-  r[P(6)] = R.c2 - I.c4;   r[P(10)] = R.c2 + I.c4;
-  i[P(6)] = I.c2 - R.c4;   i[P(10)] = I.c2 + R.c4;
-  r[P(7)] = R.c10 + I.c18; r[P(9)] = R.c10 - I.c18;
-  i[P(7)] = I.c10 + R.c18; i[P(9)] = I.c10 - R.c18;
-#undef P
-}
-
-// Leaf of size 8 at positions [o, o+8) (reference :148-212), in place.
-__device__ __forceinline__ void d_leaf8(const DConst &K, double *yr, double *yi, int o) {
-  double xr[8], xi[8], R[8], I[8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    xr[j] = yr[pidx(o + j)];
-    xi[j] = yi[pidx(o + j)];
-  }
-  d8_part(K, xr, R);
-  d8_part(K, xi, I);
-  // output stage (reference :193-209)
-#define P(j) pidx(o + (j))
-  yr[P(0)] = R[1] + R[0]; yr[P(4)] = R[1] - R[0];
-  yi[P(0)] = I[1] + I[0]; yi[P(4)] = I[1] - I[0];
-  yr[P(1)] = R[4] + I[6]; yr[P(7)] = R[4] - I[6];
-  yi[P(1)] = I[4] - R[6]; yi[P(7)] = I[4] + R[6];
-  yr[P(2)] = R[2] + I[3]; yr[P(6)] = R[2] - I[3];
-  yi[P(2)] = I[2] - R[3]; yi[P(6)] = I[2] + R[3];
-  yr[P(3)] = R[5] - I[7]; yr[P(5)] = R[5] + I[7];
-  yi[P(3)] = I[5] + R[7]; yi[P(5)] = I[5] - R[7];
-#undef P
-}
-
-// Leaves of size 4, 2, 1 (only when the whole transform has N <= 4).
-__device__ __forceinline__ void d_leaf_small(double *yr, double *yi, int o, int n) {
-  double xr[4], xi[4];
-  for (int j = 0; j < n; ++j) {
-    xr[j] = yr[pidx(o + j)];
-    xi[j] = yi[pidx(o + j)];
-  }
-  if (n == 4) {  // reference :121-147
-    const double er = xr[0] + xr[2], fr = xr[0] - xr[2], gr = xr[1] + xr[3], hr = xr[1] - xr[3];
-    const double ei = xi[0] + xi[2], fi = xi[0] - xi[2], gi = xi[1] + xi[3], hi = xi[1] - xi[3];
-    yr[pidx(o + 0)] = er + gr; yr[pidx(o + 1)] = fr + hi; yr[pidx(o + 2)] = er - gr; yr[pidx(o + 3)] = fr - hi;
-    yi[pidx(o + 0)] = ei + gi; yi[pidx(o + 1)] = fi - hr; yi[pidx(o + 2)] = ei - gi; yi[pidx(o + 3)] = fi + hr;
-  } else if (n == 2) {  // reference :108-120
-    yr[pidx(o)] = xr[0] + xr[1]; yr[pidx(o + 1)] = xr[0] - xr[1];
-    yi[pidx(o)] = xi[0] + xi[1]; yi[pidx(o + 1)] = xi[0] - xi[1];
-  }
-}
-
-// 4m2a butterfly k of a node of size n at y[off..) (reference :392-427)
-// (outputs to the planes exchanged when swap_out: the last launch of an inverse)
-__device__ __forceinline__ void d_butterfly(double *yr, double *yi, size_t stride, int off, int k, int q,
-                                            double w_r, double w_i, double scale, bool swap_out = false) {
-  double *r0 = yr + (size_t)(off + k) * stride, *i0 = yi + (size_t)(off + k) * stride;
-  const size_t qs = (size_t)q * stride;
-  const double u0r = r0[0], u1r = r0[qs], zpr = r0[2 * qs], zmr = r0[3 * qs];
-  const double u0i = i0[0], u1i = i0[qs], zpi = i0[2 * qs], zmi = i0[3 * qs];
-  const double pr = w_r * zpr + w_i * zpi, pi = w_r * zpi - w_i * zpr;
-  const double mr = w_r * zmr - w_i * zmi, mi = w_r * zmi + w_i * zmr;
-  const double sr = pr + mr, si = pi + mi, dr = pr - mr, di = pi - mi;
-  if (swap_out) {
-    double *t = r0;
-    r0 = i0;
-    i0 = t;
-  }
-  r0[0] = (u0r + sr) * scale;
-  r0[2 * qs] = (u0r - sr) * scale;
-  r0[qs] = (u1r + di) * scale;
-  r0[3 * qs] = (u1r - di) * scale;
-  i0[0] = (u0i + si) * scale;
-  i0[2 * qs] = (u0i - si) * scale;
-  i0[qs] = (u1i - dr) * scale;
-  i0[3 * qs] = (u1i + dr) * scale;
-}
-
-// 4m2a butterfly in shared memory (padded indices)
-__device__ __forceinline__ void d_butterfly_smem(double *yr, double *yi, int off, int k, int q, double w_r,
-                                                 double w_i, double scale) {
-  const int a0 = pidx(off + k), a1 = pidx(off + k + q), a2 = pidx(off + k + 2 * q), a3 = pidx(off + k + 3 * q);
-  const double u0r = yr[a0], u1r = yr[a1], zpr = yr[a2], zmr = yr[a3];
-  const double u0i = yi[a0], u1i = yi[a1], zpi = yi[a2], zmi = yi[a3];
-  const double pr = w_r * zpr + w_i * zpi, pi = w_r * zpi - w_i * zpr;
-  const double mr = w_r * zmr - w_i * zmi, mi = w_r * zmi + w_i * zmr;
-  const double sr = pr + mr, si = pi + mi, dr = pr - mr, di = pi - mi;
-  yr[a0] = (u0r + sr) * scale;
-  yr[a2] = (u0r - sr) * scale;
-  yr[a1] = (u1r + di) * scale;
-  yr[a3] = (u1r - di) * scale;
-  yi[a0] = (u0i + si) * scale;
-  yi[a2] = (u0i - si) * scale;
-  yi[a1] = (u1i - dr) * scale;
-  yi[a3] = (u1i + dr) * scale;
-}
-
-// One CTA = G instances (sub-transform root x signal) entirely in shared
-// memory.  SINGLE: N < 4096, one root per signal, G signals per CTA, all with
-// the big schedule.  Otherwise G = 1 and the CTA's root may be of size T or
-// T/2.  Per instance: gather the root's input sequence in input order
-// (coalesced reads) into DIT positions, leaves, levels, then write the outputs
-// once.  The twiddles the levels need, LUT[m*(N/T)] for m < T/4, are read
-// through L1 (a few KB, shared by all CTAs).
 template <bool SINGLE>
 __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict__ in, double *__restrict__ out, int N,
                                                         int B, const SubRoot *__restrict__ roots, int nroots, int G,
@@ -242,101 +32,13 @@ __global__ void __launch_bounds__(256, 3) d_sub_kernel(const double *__restrict_
                                                         const double *__restrict__ wr, const double *__restrict__ wi,
                                                         DConst K, double scale, int swap_in, int swap_out) {
   extern __shared__ double sm[];
-  const int Tmax = big.size;
-  const int lgT = 31 - __clz(Tmax);
-  const int istride = 2 * Tmax;  // doubles per instance: real plane, imaginary plane
-  const int tws = N / Tmax;                  // twiddle table stride of this sub-transform
-  // this CTA's instances
-  int G_here, b0;
-  SubRoot rt;
-  bool is_big = true;
   if (SINGLE) {
-    b0 = blockIdx.x * G;
-    G_here = min(G, B - b0);
-    rt = roots[0];
+    const int b0 = blockIdx.x * G;
+    d_sub_instances<true>(in, out, N, B, b0, min(G, B - b0), roots[0], big, small, wr, wi, K, scale, swap_in, swap_out,
+                          sm);
   } else {
-    const int root = blockIdx.x % nroots;
-    b0 = blockIdx.x / nroots;
-    G_here = 1;
-    rt = roots[root];
-    is_big = rt.size == Tmax;
-  }
-  const int T = rt.size;
-  const int *perm = is_big ? big.perm : small.perm;
-  const Leaf *leaves = is_big ? big.leaves : small.leaves;
-  const int nleaves = is_big ? big.nleaves : small.nleaves;
-  const int n16 = is_big ? big.nleaf16 : small.nleaf16, n8 = is_big ? big.nleaf8 : small.nleaf8;
-  const int nlevels = is_big ? big.nlevels : small.nlevels;
-  // gather: element j of instance g to DIT position perm[j]; 8 elements per
-  // thread are loaded before any is stored, so their latencies overlap
-  const int total = G_here << lgT;
-  for (int e0 = 0; e0 < total; e0 += 8 * 256) {
-    double vr[8], vi[8];
-    int dst[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int e = e0 + u * 256 + (int)threadIdx.x;
-      const int g = e >> lgT, j = e & (Tmax - 1);
-      dst[u] = -1;
-      if (e < total && (SINGLE || j < T)) {
-        int idx = rt.sn + j * rt.s;
-        if (idx < 0) idx += N;
-        const size_t b = (size_t)(b0 + g);
-        vr[u] = in[(swap_in ? (size_t)B + b : b) * N + idx];
-        vi[u] = in[(swap_in ? b : (size_t)B + b) * N + idx];
-        dst[u] = g * istride + pidx(perm[j]);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (dst[u] >= 0) {
-        sm[dst[u]] = vr[u];
-        sm[dst[u] + Tmax] = vi[u];
-      }
-  }
-  __syncthreads();
-  // leaves, grouped by size: 16-point, then 8-point, then (N <= 4 only) smaller
-  for (int e = threadIdx.x; e < G_here * nleaves; e += blockDim.x) {
-    const int g = SINGLE ? e / nleaves : 0, l = SINGLE ? e - g * nleaves : e;
-    double *yr = sm + (size_t)g * istride, *yi = yr + Tmax;
-    const Leaf lf = leaves[l];
-    if (l < n16) d_leaf16(K, yr, yi, lf.out);
-    else if (l < n16 + n8) d_leaf8(K, yr, yi, lf.out);
-    else d_leaf_small(yr, yi, lf.out, lf.n);
-  }
-  if (nlevels == 0 && scale != 1.0) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < (G_here << lgT); e += blockDim.x) {
-      const int g = e >> lgT, m = e & (Tmax - 1);
-      double *yr = sm + (size_t)g * istride, *yi = yr + Tmax;
-      yr[pidx(m)] *= scale;
-      yi[pidx(m)] *= scale;
-    }
-  }
-  // levels (the small schedule's levels are the big one's minus the last)
-  for (int lv = 0; lv < nlevels; ++lv) {
-    __syncthreads();
-    const int n = big.level_n[lv], q = n >> 2, lgq = 29 - __clz(n);
-    const int cnt = is_big ? big.level_count[lv] : small.level_count[lv];
-    const int *nodes = (is_big ? big.node_off : small.node_off) + (is_big ? big.level_start[lv] : small.level_start[lv]);
-    const int per = cnt * q;
-    const double sc = lv == nlevels - 1 ? scale : 1.0;
-    for (int e = threadIdx.x; e < G_here * per; e += blockDim.x) {
-      const int g = SINGLE ? e / per : 0, t = SINGLE ? e - g * per : e;
-      const int node = t >> lgq, k = t & (q - 1);
-      const int km = k << (lgT - (lgq + 2));  // k * (T/n)
-      double *yr = sm + (size_t)g * istride, *yi = yr + Tmax;
-      d_butterfly_smem(yr, yi, nodes[node], k, q, __ldg(wr + (size_t)km * tws), __ldg(wi + (size_t)km * tws), sc);
-    }
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < (G_here << lgT); e += blockDim.x) {
-    const int g = e >> lgT, m = e & (Tmax - 1);
-    if (!SINGLE && m >= T) continue;
-    const int b = b0 + g;
-    const double *yr = sm + (size_t)g * istride, *yi = yr + Tmax;
-    out[(swap_out ? (size_t)B + b : (size_t)b) * N + rt.out + m] = yr[pidx(m)];
-    out[(swap_out ? (size_t)b : (size_t)B + b) * N + rt.out + m] = yi[pidx(m)];
+    d_sub_instances<false>(in, out, N, B, blockIdx.x / nroots, 1, roots[blockIdx.x % nroots], big, small, wr, wi, K,
+                           scale, swap_in, swap_out, sm);
   }
 }
 

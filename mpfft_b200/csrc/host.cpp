@@ -26,8 +26,10 @@
 #include <atomic>
 #include <condition_variable>
 #include <thread>
+#include <tuple>
 #include <vector>
 
+#include <sys/stat.h>
 #include <unistd.h>
 #if defined(__x86_64__)
 #include <immintrin.h>
@@ -689,7 +691,17 @@ static int mp_plan_init_nd(mpfft_mp_plan *p, int rank, const unsigned long *dims
 //   double-double (about 106 bits)  48 < P <= 98
 //   quad-double (about 212 bits)  98 < P <= 200
 // Larger precisions keep the limb kernels.
-static int float_form_for(long P) {
+// With MPFFT_PLAN_NATIVE_TIERS instead, P picks the smallest word format that
+// holds P bits (float-float 48, FP64 53, double-double 106, quad-double 212)
+// and the result carries that tier's own error, about log2(N) 2^-(bits-2).
+static int float_form_for(long P, bool native = false) {
+  if (native) {
+    if (P <= 48) return MPFFT_FORM_FLOAT_FLOAT;
+    if (P <= 53) return MPFFT_FORM_DOUBLE;
+    if (P <= 106) return MPFFT_FORM_DOUBLE_DOUBLE;
+    if (P <= 212) return MPFFT_FORM_QUAD_DOUBLE;
+    return -1;
+  }
   if (P <= 40) return MPFFT_FORM_FLOAT_FLOAT;
   if (P <= 48) return MPFFT_FORM_DOUBLE;
   if (P <= 98) return MPFFT_FORM_DOUBLE_DOUBLE;
@@ -697,11 +709,11 @@ static int float_form_for(long P) {
   return -1;
 }
 
-static int d_plan_init(mpfft_d_plan *p, unsigned long n);
-static int d_plan_init_tier(mpfft_d_plan *p, unsigned long n, int tier);
+static int d_plan_init(mpfft_d_plan *p, unsigned long n, int sub_max = 0);
+static int d_plan_init_tier(mpfft_d_plan *p, unsigned long n, int tier, int sub_max = 0);
 
-static int mp_plan_attach_float_tier(mpfft_mp_plan *p) {
-  const int form = float_form_for(p->P);
+static int mp_plan_attach_float_tier(mpfft_mp_plan *p, bool native) {
+  const int form = float_form_for(p->P, native);
   if (form < 0 || p->rank > 1 || p->real || p->host_only) return MPFFT_OK;
   std::unique_ptr<mpfft_d_plan> f(new (std::nothrow) mpfft_d_plan);
   if (!f) return set_err(MPFFT_ENOMEM, "out of host memory");
@@ -1330,14 +1342,16 @@ static int build_sub(mpfft_d_plan *p, int size, SubSchedule &S, int leaf_max = 1
   return MPFFT_OK;
 }
 
-static int d_plan_init(mpfft_d_plan *p, unsigned long n) {
+// sub_max: largest shared-memory sub-transform (0: the default kDSubMax; the
+// results do not depend on it, only where each butterfly runs)
+static int d_plan_init(mpfft_d_plan *p, unsigned long n, int sub_max) {
   if (!is_pow2(n)) return set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
   if (n > (1UL << 28)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
   if (int e = device_ready()) return e;
   p->N = n;
   p->tabs.N = (int)n;
   // cut the tree at T points: maximal nodes of size <= T run in shared memory
-  const int T = (int)std::min<unsigned long>(n, kDSubMax);
+  const int T = (int)std::min<unsigned long>(n, sub_max > 0 ? sub_max : kDSubMax);
   {
     HostTree t;
     walk(t, (int)n, 1, 0, 0, T);
@@ -1559,7 +1573,7 @@ static int d_execute_impl(mpfft_d_plan *p, unsigned long batch, const double *in
 // points; cos and sin of 2 pi k/n computed by MPFR at 320 bits and split into
 // the tier's words (each the nearest double to what the words above leave;
 // float-float keeps one double: its products are formed in FP64).
-static int d_plan_init_tier(mpfft_d_plan *p, unsigned long n, int tier) {
+static int d_plan_init_tier(mpfft_d_plan *p, unsigned long n, int tier, int sub_max) {
   if (!is_pow2(n)) return set_err(MPFFT_EINVAL, "n=%lu is not a power of two", n);
   if (n > (1UL << 26)) return set_err(MPFFT_EUNSUPPORTED, "n=%lu too large", n);
   if (int e = device_ready()) return e;
@@ -1567,7 +1581,7 @@ static int d_plan_init_tier(mpfft_d_plan *p, unsigned long n, int tier) {
   p->tier = tier;
   p->dd = tier == kTierDD;
   p->tabs.N = (int)n;
-  const int T = (int)std::min<unsigned long>(n, (unsigned long)tier_sub_max(tier));
+  const int T = (int)std::min<unsigned long>(n, (unsigned long)(sub_max > 0 ? sub_max : tier_sub_max(tier)));
   {
     HostTree t;
     walk(t, (int)n, 1, 0, 0, T);
@@ -1690,14 +1704,54 @@ static int d_execute_real(mpfft_d_plan *p, bool forward, unsigned long batch, co
 
 static void d_plan_delete(mpfft_d_plan *p) { delete p; }
 
+// The words of one real value x in a compensated tier (K words, floats when
+// fl): the nearest word, then the nearest word to what is left, ... (exact
+// down to the last word), word h stored at dst[at + h*stride].  t: scratch
+// mpfr_t.  Returns 0, 1 for NaN/infinity, 2 for an exponent outside
+// [emin, emax] (the window the words represent without underflow or overflow
+// over N-point growth).
+static inline int mpfr_to_words(mpfr_srcptr x, mpfr_ptr t, int K, bool fl, long emin, long emax, void *dst,
+                                size_t at, size_t stride) {
+  if (!mpfr_number_p(x)) return 1;
+  if (!mpfr_zero_p(x) && (x->_mpfr_exp < emin || x->_mpfr_exp > emax)) return 2;
+  if (mpfr_get_prec(t) < mpfr_get_prec(x)) mpfr_set_prec(t, mpfr_get_prec(x));
+  mpfr_set(t, x, MPFR_RNDN);  // exact
+  for (int h = 0; h < K; ++h) {
+    const double w = fl ? (double)(float)mpfr_get_d(t, MPFR_RNDN) : mpfr_get_d(t, MPFR_RNDN);
+    mpfr_sub_d(t, t, w, MPFR_RNDN);  // exact: the part of t below w
+    if (fl) static_cast<float *>(dst)[at + (size_t)h * stride] = (float)w;
+    else static_cast<double *>(dst)[at + (size_t)h * stride] = w;
+  }
+  return 0;
+}
+
+// y = (sum of the K words at src[at + h*stride]) * 2^-shift, rounded to nearest
+// into y's precision; acc: a 320-bit scratch mpfr_t (the sum of a tier's words
+// is exact at 320 bits)
+static inline void words_to_mpfr(const void *src, size_t at, size_t stride, int K, bool fl, long shift, mpfr_ptr acc,
+                                 mpfr_ptr y) {
+  mpfr_set_zero(acc, 1);
+  for (int h = 0; h < K; ++h)
+    mpfr_add_d(acc, acc,
+               fl ? (double)static_cast<const float *>(src)[at + (size_t)h * stride]
+                  : static_cast<const double *>(src)[at + (size_t)h * stride],
+               MPFR_RNDN);
+  mpfr_mul_2si(acc, acc, -shift, MPFR_RNDN);
+  mpfr_set(y, acc, MPFR_RNDN);
+}
+
+static inline void tier_window(const mpfft_d_plan *f, long *emin, long *emax) {
+  const bool fl = d_word_bytes(f) == 4;
+  *emin = fl ? -100 : -700;
+  *emax = fl ? 90 : 900;
+}
+
 // A transform through the plan's compensated floating-point tier: every mpfr_t
-// input is split on the host into the tier's words (the nearest word, then the
-// nearest word to what is left, ...; exact down to the last word), the tier's
-// kernels run, and each output is the words' sum (at 320 bits, exact for
-// these words) times 2^-fadj, rounded to nearest into the output's precision.
-// Returns kFloatOutOfRange, before writing any output, when an input exponent
-// lies outside the window the tier's words represent without underflow or
-// overflow over N-point growth; the caller then runs the limb kernels.
+// input is split on the host into the tier's words (mpfr_to_words), the
+// tier's kernels run, and each output is the words' sum times 2^-fadj rounded
+// into the output's precision (words_to_mpfr).  Returns kFloatOutOfRange,
+// before writing any output, when an input exponent lies outside the tier's
+// window; the caller then runs the limb kernels.
 static int mp_execute_float(mpfft_mp_plan *p, unsigned long batch, const IoShape &ii, mpfr_t *inr, mpfr_t *ini,
                             const IoShape &oo, mpfr_t *outr, mpfr_t *outi, long fadj) {
   mpfft_d_plan *f = p->fplan;
@@ -1708,61 +1762,39 @@ static int mp_execute_float(mpfft_mp_plan *p, unsigned long batch, const IoShape
   if (int e = d_reserve(f, batch)) return e;
   const int K = d_words(f);
   const bool fl = d_word_bytes(f) == 4;
-  const long emin = fl ? -100 : -700, emax = fl ? 90 : 900;
+  long emin, emax;
+  tier_window(f, &emin, &emax);
   const size_t hplane = (size_t)N * batch;
-  float *hf = reinterpret_cast<float *>(f->h_in);
-  std::atomic<int> nonfin{0}, range{0};
+  std::atomic<int> status{0};
   parallel_for((long)hplane, 1024, [&](long a0, long a1) {
     mpfr_t t;
     mpfr_init2(t, 64);
+    int st = 0;
     for (long u = a0; u < a1; ++u) {
       const unsigned long b = (unsigned long)u / N, q = (unsigned long)u % N;
-      for (int c = 0; c < 2; ++c) {
-        mpfr_srcptr x = elem(c ? ini : inr, c, b, ii, q);
-        const size_t at = ((size_t)c * K * batch + b) * N + q;
-        if (!mpfr_number_p(x)) {
-          nonfin.store(1, std::memory_order_relaxed);
-          continue;
-        }
-        if (!mpfr_zero_p(x) && (x->_mpfr_exp < emin || x->_mpfr_exp > emax)) {
-          range.store(1, std::memory_order_relaxed);
-          continue;
-        }
-        if (mpfr_get_prec(t) < mpfr_get_prec(x)) mpfr_set_prec(t, mpfr_get_prec(x));
-        mpfr_set(t, x, MPFR_RNDN);  // exact
-        for (int h = 0; h < K; ++h) {
-          const double w = fl ? (double)(float)mpfr_get_d(t, MPFR_RNDN) : mpfr_get_d(t, MPFR_RNDN);
-          mpfr_sub_d(t, t, w, MPFR_RNDN);  // exact: the part of t below w
-          if (fl) hf[at + (size_t)h * hplane] = (float)w;
-          else f->h_in[at + (size_t)h * hplane] = w;
-        }
-      }
+      for (int c = 0; c < 2; ++c)
+        st |= mpfr_to_words(elem(c ? ini : inr, c, b, ii, q), t, K, fl, emin, emax, f->h_in,
+                            ((size_t)c * K * batch + b) * N + q, hplane);
     }
     mpfr_clear(t);
+    if (st) status.fetch_or(st);
   });
-  if (range.load()) return kFloatOutOfRange;
-  if (nonfin.load()) return set_err(MPFFT_ENONFINITE, "input holds NaN or infinity");
+  if (status.load() & 2) return kFloatOutOfRange;
+  if (status.load() & 1) return set_err(MPFFT_ENONFINITE, "input holds NaN or infinity");
   const size_t bytes = (size_t)2 * K * hplane * d_word_bytes(f);
   CUDA_TRY(cudaMemcpyAsync(f->d_in, f->h_in, bytes, cudaMemcpyHostToDevice, f->stream));
   if (f->tier < 0) CUDA_TRY(d_run_transform(f->tabs, f->d_in, f->d_out, (int)batch, 1.0, f->stream));
   else CUDA_TRY(tier_run_transform(f->tier, f->tabs, f->d_in, f->d_out, (int)batch, 1.0, f->stream));
   CUDA_TRY(cudaMemcpyAsync(f->h_out, f->d_out, bytes, cudaMemcpyDeviceToHost, f->stream));
   CUDA_TRY(cudaStreamSynchronize(f->stream));
-  const float *of = reinterpret_cast<const float *>(f->h_out);
   parallel_for((long)hplane, 1024, [&](long a0, long a1) {
     mpfr_t acc;
     mpfr_init2(acc, 320);
     for (long u = a0; u < a1; ++u) {
       const unsigned long b = (unsigned long)u / N, q = (unsigned long)u % N;
-      for (int c = 0; c < 2; ++c) {
-        const size_t at = ((size_t)c * K * batch + b) * N + q;
-        mpfr_set_zero(acc, 1);
-        for (int h = 0; h < K; ++h)
-          mpfr_add_d(acc, acc, fl ? (double)of[at + (size_t)h * hplane] : f->h_out[at + (size_t)h * hplane],
-                     MPFR_RNDN);
-        mpfr_mul_2si(acc, acc, -fadj, MPFR_RNDN);
-        mpfr_set(elem(c ? outi : outr, c, b, oo, q), acc, MPFR_RNDN);
-      }
+      for (int c = 0; c < 2; ++c)
+        words_to_mpfr(f->h_out, ((size_t)c * K * batch + b) * N + q, hplane, K, fl, fadj, acc,
+                      elem(c ? outi : outr, c, b, oo, q));
     }
     mpfr_clear(acc);
   });
@@ -1868,8 +1900,8 @@ MPFFT_API int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, 
   if (flags & MPFFT_PLAN_NO_TENSOR) p->tabs.tc = 0;
   else if (flags & MPFFT_PLAN_TENSOR) p->tabs.tc = 2;
   if (!p->host_only && mp_tc_used(p->tabs, p->L)) p->form = MPFFT_FORM_TENSOR;
-  if (flags & MPFFT_PLAN_FLOAT_TIERS)
-    if (int e = mp_plan_attach_float_tier(p.get())) return e;
+  if (flags & (MPFFT_PLAN_FLOAT_TIERS | MPFFT_PLAN_NATIVE_TIERS))
+    if (int e = mp_plan_attach_float_tier(p.get(), (flags & MPFFT_PLAN_NATIVE_TIERS) != 0)) return e;
   *plan = p.release();
   return set_err(MPFFT_OK, "");
 }
@@ -2358,6 +2390,16 @@ MPFFT_API int mpfft_diag_tc_error(void) {
   return code ? set_err(MPFFT_ECUDA, "a tensor-core wait expired (code %d)", code) : set_err(MPFFT_OK, "");
 }
 
+MPFFT_API int mpfft_diag_tc_int8_rate(double *macs_per_s) {
+  if (!macs_per_s) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (int e = device_ready()) return e;
+  CUDA_TRY(mp_tc_int8_rate(macs_per_s));
+  int code = 0;
+  CUDA_TRY(mp_tc_take_error(&code));
+  if (code) return set_err(MPFFT_ECUDA, "a tensor-core wait expired (code %d)", code);
+  return set_err(MPFFT_OK, "");
+}
+
 MPFFT_API int mpfft_diag_imad_rate(int wide, double *ops_per_s) {
   if (!ops_per_s) return set_err(MPFFT_EINVAL, "NULL argument");
   if (int e = device_ready()) return e;
@@ -2408,3 +2450,528 @@ MPFFT_API int mpfft_mp_execute_significands_static(const mpfft_mp_plan *plan, un
 }
 
 MPFFT_API size_t mpfft_static_scratch_bytes(void) { return static_scratch_bytes(); }
+
+// ===========================================================================
+// uneven batches as one graph launch of persistent work-queue kernels
+// ===========================================================================
+
+namespace mpfft {
+
+// process-wide caches of FP64 / compensated-tier plans by (n, tier, sub size)
+static std::map<std::tuple<unsigned long, int, int>, std::unique_ptr<mpfft_d_plan>> g_ft_cache;
+
+static mpfft_d_plan *ft_cached(unsigned long n, int tier, int sub_max) {
+  std::lock_guard<std::mutex> g(g_cache_mu);
+  const auto key = std::make_tuple(n, tier, sub_max);
+  auto it = g_ft_cache.find(key);
+  if (it != g_ft_cache.end()) return it->second.get();
+  std::unique_ptr<mpfft_d_plan> p(new mpfft_d_plan);
+  if ((tier < 0 ? d_plan_init(p.get(), n, sub_max) : d_plan_init_tier(p.get(), n, tier, sub_max)) != MPFFT_OK)
+    return nullptr;
+  auto *raw = p.get();
+  g_ft_cache[key] = std::move(p);
+  return raw;
+}
+
+static int form_family(int form) {
+  switch (form) {
+    case MPFFT_FORM_DOUBLE: return kQueueDouble;
+    case MPFFT_FORM_DOUBLE_DOUBLE: return kQueueTierDD;
+    case MPFFT_FORM_QUAD_DOUBLE: return kQueueTierQD;
+    case MPFFT_FORM_FLOAT_FLOAT: return kQueueTierFF;
+    default: return kQueueLimbs;
+  }
+}
+static int family_tier(int fam) {
+  return fam == kQueueTierDD ? kTierDD : fam == kQueueTierQD ? kTierQD : fam == kQueueTierFF ? kTierFF : -1;
+}
+static int family_default_sub(int fam) { return fam == kQueueDouble ? kDSubMax : tier_sub_max(family_tier(fam)); }
+
+// relative cost of one point-level of each form, for largest-first ordering
+static double form_cost(int fam, int L) {
+  switch (fam) {
+    case kQueueDouble: return 1.0;
+    case kQueueTierFF: return 2.0;
+    case kQueueTierDD: return 8.0;
+    case kQueueTierQD: return 60.0;
+    default: return 0.6 * L * L + 4.0 * L;
+  }
+}
+
+}  // namespace mpfft
+
+struct mpfft_batch_plan {
+  struct Sig {
+    unsigned long n = 0;
+    long prec = 0;
+    int form = 0, L = 0, queue = 0, tab = 0;
+    size_t off = 0, bytes = 0;  // place in the arenas
+    mpfft_mp_plan *mp = nullptr;
+    mpfft_d_plan *fp = nullptr;
+  };
+  struct Queue {
+    int family = 0, L = 0;  // L: limb count of a limb queue
+    int threads = 256, sub = 0, ctas = 1;
+    std::vector<unsigned long> sigs;  // largest first
+    QueueItem *d_items = nullptr;
+  };
+  std::vector<Sig> sig;
+  std::vector<Queue> queues;
+  std::vector<QueueTables> tabs;
+  QueueTables *d_tabs = nullptr;
+  int *d_heads = nullptr;
+  unsigned char *d_in = nullptr, *d_out = nullptr, *h_in = nullptr, *h_out = nullptr;
+  size_t arena = 0;
+  std::vector<long> exps;  // limb signals: block exponents of the last host-array call
+  cudaStream_t stream = nullptr;
+  std::vector<cudaStream_t> qstreams;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> joins;
+  cudaGraphExec_t graph = nullptr;
+  int device = -1;
+  std::mutex mu;
+  void free_graph() {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+  }
+  ~mpfft_batch_plan() {
+    free_graph();
+    for (auto &q : queues)
+      if (q.d_items) cudaFree(q.d_items);
+    for (void *p : {(void *)d_tabs, (void *)d_heads, (void *)d_in, (void *)d_out})
+      if (p) cudaFree(p);
+    for (void *p : {(void *)h_in, (void *)h_out})
+      if (p) cudaFreeHost(p);
+    for (cudaStream_t s : qstreams) cudaStreamDestroy(s);
+    for (cudaEvent_t e : joins) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace mpfft {
+
+// (Re)build a queue's tables and items for its current sub size, and its grid.
+static int batch_build_queue(mpfft_batch_plan *bp, int qi) {
+  auto &Q = bp->queues[qi];
+  std::vector<QueueItem> items;
+  for (unsigned long i : Q.sigs) {
+    auto &s = bp->sig[i];
+    if (Q.family != kQueueLimbs) {
+      s.fp = ft_cached(s.n, family_tier(Q.family), Q.sub);
+      if (!s.fp) return g_err;
+      bp->tabs[s.tab].ft = s.fp->tabs;
+    }
+    items.push_back(QueueItem{bp->d_in + s.off, bp->d_out + s.off, bp->d_tabs + s.tab});
+  }
+  if (!Q.d_items) CUDA_TRY(cudaMalloc(&Q.d_items, std::max<size_t>(1, items.size()) * sizeof(QueueItem)));
+  CUDA_TRY(cudaMemcpy(Q.d_items, items.data(), items.size() * sizeof(QueueItem), cudaMemcpyHostToDevice));
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, bp->device));
+  CUDA_TRY(queue_prepare(Q.family, Q.L));
+  Q.ctas = (int)std::min<size_t>(Q.sigs.size(), (size_t)sms * queue_ctas_per_sm(Q.family, Q.L, Q.threads));
+  return MPFFT_OK;
+}
+
+// Capture the whole batch as one graph: zero the queue counters, fork one
+// branch per queue, launch its persistent kernel, join.
+static int batch_capture(mpfft_batch_plan *bp) {
+  bp->free_graph();
+  CUDA_TRY(cudaMemcpy(bp->d_tabs, bp->tabs.data(), bp->tabs.size() * sizeof(QueueTables), cudaMemcpyHostToDevice));
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(cudaStreamBeginCapture(bp->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaMemsetAsync(bp->d_heads, 0, bp->queues.size() * sizeof(int), bp->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(bp->fork, bp->stream);
+  for (size_t q = 0; q < bp->queues.size() && e == cudaSuccess; ++q) {
+    const auto &Q = bp->queues[q];
+    e = cudaStreamWaitEvent(bp->qstreams[q], bp->fork, 0);
+    if (e == cudaSuccess)
+      e = queue_launch(Q.family, Q.L, Q.d_items, (int)Q.sigs.size(), bp->d_heads + q, Q.ctas, Q.threads, 1.0,
+                       bp->qstreams[q]);
+    if (e == cudaSuccess) e = cudaEventRecord(bp->joins[q], bp->qstreams[q]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(bp->stream, bp->joins[q], 0);
+  }
+  const cudaError_t ce = cudaStreamEndCapture(bp->stream, &g);
+  if (e == cudaSuccess) e = ce;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&bp->graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    bp->graph = nullptr;
+    cudaGetLastError();
+    return set_err(MPFFT_ECUDA, "capturing the batch graph: %s", cudaGetErrorString(e));
+  }
+  return MPFFT_OK;
+}
+
+// ---- autotuning of the queue launches --------------------------------------
+//
+// Per queue the choices are the CTA size and, for the floating forms, the
+// largest shared-memory sub-transform (a smaller one lets more CTAs share an
+// SM at the price of more levels in global memory); neither changes any
+// result.  mpfft_batch_autotune times every candidate on the batch's own
+// queues and records the fastest per (device, queue kind, length mix) in a
+// JSON file -- MPFFT_AUTOTUNE_FILE, else $XDG_CACHE_HOME/mpfft_b200/autotune.json,
+// else ~/.cache/mpfft_b200/autotune.json -- which later plans read.
+
+static std::string tune_path() {
+  if (const char *p = getenv("MPFFT_AUTOTUNE_FILE")) return p;
+  std::string base;
+  if (const char *x = getenv("XDG_CACHE_HOME")) base = x;
+  else if (const char *h = getenv("HOME")) base = std::string(h) + "/.cache";
+  else return "";
+  return base + "/mpfft_b200/autotune.json";
+}
+
+static std::string tune_key(const mpfft_batch_plan *bp, int qi) {
+  const auto &Q = bp->queues[qi];
+  cudaDeviceProp prop;
+  std::string dev = cudaGetDeviceProperties(&prop, bp->device) == cudaSuccess ? prop.name : "gpu";
+  for (auto &c : dev)
+    if (c == '"' || c == ' ') c = '_';
+  // length mix: the signal count per log2 N
+  int hist[32] = {};
+  for (unsigned long i : Q.sigs) ++hist[ilog2(bp->sig[i].n)];
+  std::string mix;
+  for (int l = 0; l < 32; ++l)
+    if (hist[l]) mix += std::to_string(l) + "x" + std::to_string(hist[l]) + ".";
+  return dev + "/" + std::to_string(Q.family) + "/" + std::to_string(Q.L) + "/" + mix;
+}
+
+// entries "key": [threads, sub] of the tune file
+static std::map<std::string, std::pair<int, int>> tune_load() {
+  std::map<std::string, std::pair<int, int>> m;
+  const std::string path = tune_path();
+  FILE *f = path.empty() ? nullptr : fopen(path.c_str(), "r");
+  if (!f) return m;
+  std::string txt;
+  char buf[4096];
+  for (size_t k; (k = fread(buf, 1, sizeof buf, f)) > 0;) txt.append(buf, k);
+  fclose(f);
+  for (size_t p = 0; (p = txt.find('"', p)) != std::string::npos;) {
+    const size_t e = txt.find('"', p + 1);
+    if (e == std::string::npos) break;
+    const std::string key = txt.substr(p + 1, e - p - 1);
+    int t = 0, s = 0;
+    if (sscanf(txt.c_str() + e + 1, " : [ %d , %d ]", &t, &s) == 2) m[key] = std::make_pair(t, s);
+    p = e + 1;
+  }
+  return m;
+}
+
+static void tune_save(const std::map<std::string, std::pair<int, int>> &m) {
+  const std::string path = tune_path();
+  if (path.empty()) return;
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos) {  // create the directory chain
+    for (size_t p = 1; p <= slash; ++p)
+      if (path[p] == '/' || p == slash) mkdir(path.substr(0, p == slash ? slash : p).c_str(), 0755);
+  }
+  const std::string tmp = path + ".tmp" + std::to_string(getpid());
+  FILE *f = fopen(tmp.c_str(), "w");
+  if (!f) return;
+  fprintf(f, "{\n");
+  size_t k = 0;
+  for (auto &kv : m) fprintf(f, "  \"%s\": [%d, %d]%s\n", kv.first.c_str(), kv.second.first, kv.second.second,
+                             ++k < m.size() ? "," : "");
+  fprintf(f, "}\n");
+  fclose(f);
+  rename(tmp.c_str(), path.c_str());
+}
+
+}  // namespace mpfft
+
+MPFFT_API int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long count, const unsigned long *n,
+                                      const long *prec, unsigned flags) {
+  if (!plan || !n || !prec) return set_err(MPFFT_EINVAL, "NULL argument");
+  *plan = nullptr;
+  if (count == 0) return set_err(MPFFT_EINVAL, "empty batch");
+  if (int e = device_ready()) return e;
+  std::unique_ptr<mpfft_batch_plan> bp(new (std::nothrow) mpfft_batch_plan);
+  if (!bp) return set_err(MPFFT_ENOMEM, "out of host memory");
+  CUDA_TRY(cudaGetDevice(&bp->device));
+  bp->sig.resize(count);
+  std::map<std::pair<int, int>, int> qindex;              // (family, L) -> queue
+  std::map<std::tuple<int, int, unsigned long>, int> tindex;  // (family, L, n) -> tables
+  for (unsigned long i = 0; i < count; ++i) {
+    auto &s = bp->sig[i];
+    if (!is_pow2(n[i])) return set_err(MPFFT_EINVAL, "n[%lu]=%lu is not a power of two", i, n[i]);
+    if (prec[i] < 2) return set_err(MPFFT_EINVAL, "signal %lu: precision %ld < 2", i, prec[i]);
+    if (n[i] > (1UL << 22)) return set_err(MPFFT_EUNSUPPORTED, "signal %lu: n=%lu above the queue limit 2^22", i, n[i]);
+    s.n = n[i];
+    s.prec = prec[i];
+    const int ff = (flags & MPFFT_PLAN_NATIVE_TIERS)  ? float_form_for(prec[i], true)
+                   : (flags & MPFFT_PLAN_FLOAT_TIERS) ? float_form_for(prec[i])
+                                                      : -1;
+    int fam;
+    if (ff >= 0) {
+      s.form = ff;
+      fam = form_family(ff);
+      const int K = fam == kQueueDouble ? 1 : tier_words(family_tier(fam));
+      const size_t wb = fam == kQueueDouble ? 8 : tier_word_bytes(family_tier(fam));
+      s.bytes = (size_t)2 * K * s.n * wb;
+    } else {
+      s.form = MPFFT_FORM_LIMBS;
+      fam = kQueueLimbs;
+      s.L = mp_limbs_for(s.n, s.prec);
+      if (s.L > kMaxLimbs)
+        return set_err(MPFFT_EUNSUPPORTED, "signal %lu: %d limbs; the queue kernels take up to %d", i, s.L,
+                       kMaxLimbs);
+      s.mp = mp_cached(s.n, s.prec);
+      if (!s.mp) return g_err;
+      s.bytes = (size_t)2 * s.L * s.n * 4;
+    }
+    const auto qk = std::make_pair(fam, s.L);
+    if (!qindex.count(qk)) {
+      qindex[qk] = (int)bp->queues.size();
+      mpfft_batch_plan::Queue Q;
+      Q.family = fam;
+      Q.L = s.L;
+      Q.threads = fam == kQueueLimbs ? 128 : 256;
+      Q.sub = fam == kQueueLimbs ? 0 : family_default_sub(fam);
+      bp->queues.push_back(Q);
+    }
+    s.queue = qindex[qk];
+    const auto tk = std::make_tuple(fam, s.L, s.n);
+    if (!tindex.count(tk)) {
+      tindex[tk] = (int)bp->tabs.size();
+      QueueTables t;
+      t.N = (int)s.n;
+      if (fam == kQueueLimbs) {
+        t.tree = s.mp->tabs;
+        t.tw = s.mp->tabs.tw;
+        t.dneg = s.mp->tabs.dneg;
+      }
+      bp->tabs.push_back(t);
+    }
+    s.tab = tindex[tk];
+    bp->queues[s.queue].sigs.push_back(i);
+  }
+  // largest first within each queue; arena offsets queue by queue (256-byte aligned)
+  for (auto &Q : bp->queues) {
+    std::stable_sort(Q.sigs.begin(), Q.sigs.end(), [&](unsigned long a, unsigned long b) {
+      const auto &x = bp->sig[a], &y = bp->sig[b];
+      return (double)x.n * (ilog2(x.n) + 1) > (double)y.n * (ilog2(y.n) + 1);
+    });
+    for (unsigned long i : Q.sigs) {
+      bp->sig[i].off = bp->arena;
+      bp->arena += (bp->sig[i].bytes + 255) & ~(size_t)255;
+    }
+  }
+  (void)form_cost;
+  CUDA_TRY(cudaMalloc(&bp->d_tabs, bp->tabs.size() * sizeof(QueueTables)));
+  CUDA_TRY(cudaMalloc(&bp->d_heads, bp->queues.size() * sizeof(int)));
+  if (dev_alloc((void **)&bp->d_in, bp->arena) != cudaSuccess || dev_alloc((void **)&bp->d_out, bp->arena) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(MPFFT_ENOMEM, "cannot allocate %zu-byte signal arenas", bp->arena);
+  }
+  CUDA_TRY(cudaStreamCreateWithFlags(&bp->stream, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&bp->fork, cudaEventDisableTiming));
+  const auto tuned = tune_load();
+  for (size_t q = 0; q < bp->queues.size(); ++q) {
+    cudaStream_t s;
+    cudaEvent_t e;
+    CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    bp->qstreams.push_back(s);
+    CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    bp->joins.push_back(e);
+    auto it = tuned.find(tune_key(bp.get(), (int)q));
+    if (it != tuned.end()) {
+      bp->queues[q].threads = it->second.first;
+      if (bp->queues[q].family != kQueueLimbs) bp->queues[q].sub = it->second.second;
+    }
+    if (int e2 = batch_build_queue(bp.get(), (int)q)) return e2;
+  }
+  if (int e = batch_capture(bp.get())) return e;
+  *plan = bp.release();
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_batch_plan_destroy(mpfft_batch_plan *plan) {
+  delete plan;
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_batch_signal_format(const mpfft_batch_plan *plan, unsigned long i, int *form, int *words,
+                                        size_t *offset, size_t *bytes) {
+  if (!plan || !form || !words || !offset || !bytes) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (i >= plan->sig.size()) return set_err(MPFFT_EINVAL, "signal %lu out of range", i);
+  const auto &s = plan->sig[i];
+  *form = s.form;
+  *words = s.form == MPFFT_FORM_LIMBS ? s.L : (s.form == MPFFT_FORM_DOUBLE ? 1 : tier_words(family_tier(form_family(s.form))));
+  *offset = s.off;
+  *bytes = s.bytes;
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_batch_arenas(const mpfft_batch_plan *plan, void **d_in, void **d_out, size_t *bytes) {
+  if (!plan || !d_in || !d_out || !bytes) return set_err(MPFFT_EINVAL, "NULL argument");
+  *d_in = plan->d_in;
+  *d_out = plan->d_out;
+  *bytes = plan->arena;
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_batch_execute_device(mpfft_batch_plan *plan, void *stream) {
+  if (!plan) return set_err(MPFFT_EINVAL, "NULL argument");
+  std::lock_guard<std::mutex> g(plan->mu);
+  CUDA_TRY(cudaGraphLaunch(plan->graph, (cudaStream_t)stream));
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_batch_execute(mpfft_batch_plan *plan, mpfr_t *const *inr, mpfr_t *const *ini,
+                                  mpfr_t *const *outr, mpfr_t *const *outi, unsigned flags) {
+  if (!plan || !inr || !ini || !outr || !outi) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (flags & ~(MPFFT_SCALED | MPFFT_INVERSE)) return set_err(MPFFT_EINVAL, "flags 0x%x", flags);
+  if (flags & MPFFT_INVERSE) {  // ifft(X) = swap(FFT(swap(X)))
+    std::swap(inr, ini);
+    std::swap(outr, outi);
+  }
+  std::lock_guard<std::mutex> g(plan->mu);
+  const unsigned long count = plan->sig.size();
+  for (unsigned long i = 0; i < count; ++i)
+    if (!inr[i] || !ini[i] || !outr[i] || !outi[i]) return set_err(MPFFT_EINVAL, "NULL array of signal %lu", i);
+  if (!plan->h_in) {
+    if (host_alloc((void **)&plan->h_in, plan->arena) != cudaSuccess ||
+        host_alloc((void **)&plan->h_out, plan->arena) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(MPFFT_ENOMEM, "cannot allocate %zu bytes of pinned staging", plan->arena);
+    }
+  }
+  plan->exps.assign(count, 0);
+  // inputs -> arena layout (limb planes with a block exponent, or tier words)
+  std::atomic<int> status{0};
+  std::atomic<unsigned long> bad_sig{0};
+  parallel_for((long)count, 1, [&](long a, long b) {
+    mpfr_t t;
+    mpfr_init2(t, 64);
+    for (long i = a; i < b; ++i) {
+      const auto &s = plan->sig[i];
+      IoShape io = io_signals(s.n, 1);
+      if (s.form == MPFFT_FORM_LIMBS) {
+        mpfr_t *bi[2] = {inr[i], ini[i]};
+        io.base[0] = &bi[0];
+        io.base[1] = &bi[1];
+        if (mp_pack_impl(s.mp, 1, io, nullptr, nullptr, reinterpret_cast<uint32_t *>(plan->h_in + s.off),
+                         &plan->exps[i]) != MPFFT_OK) {
+          status.fetch_or(1);
+          bad_sig.store(i);
+        }
+      } else {
+        const int K = s.form == MPFFT_FORM_DOUBLE ? 1 : tier_words(family_tier(form_family(s.form)));
+        const bool fl = s.form == MPFFT_FORM_FLOAT_FLOAT;
+        long emin, emax;
+        tier_window(s.fp, &emin, &emax);
+        int st = 0;
+        for (unsigned long q = 0; q < s.n; ++q)
+          for (int c = 0; c < 2; ++c)
+            st |= mpfr_to_words((c ? ini : inr)[i][q], t, K, fl, emin, emax, plan->h_in + s.off,
+                                (size_t)c * K * s.n + q, s.n);
+        if (st) {
+          status.fetch_or(st);
+          bad_sig.store(i);
+        }
+      }
+    }
+    mpfr_clear(t);
+  });
+  if (status.load() & 1) return set_err(MPFFT_ENONFINITE, "signal %lu holds NaN or infinity", bad_sig.load());
+  if (status.load() & 2)
+    return set_err(MPFFT_EUNSUPPORTED, "signal %lu has exponents outside its floating tier's window",
+                   bad_sig.load());
+  CUDA_TRY(cudaMemcpyAsync(plan->d_in, plan->h_in, plan->arena, cudaMemcpyHostToDevice, plan->stream));
+  CUDA_TRY(cudaGraphLaunch(plan->graph, plan->stream));
+  CUDA_TRY(cudaMemcpyAsync(plan->h_out, plan->d_out, plan->arena, cudaMemcpyDeviceToHost, plan->stream));
+  CUDA_TRY(cudaStreamSynchronize(plan->stream));
+  parallel_for((long)count, 1, [&](long a, long b) {
+    mpfr_t acc;
+    mpfr_init2(acc, 320);
+    for (long i = a; i < b; ++i) {
+      const auto &s = plan->sig[i];
+      const long shift = (flags & MPFFT_SCALED) ? ilog2(s.n) : 0;
+      IoShape io = io_signals(s.n, 1);
+      if (s.form == MPFFT_FORM_LIMBS) {
+        mpfr_t *bo[2] = {outr[i], outi[i]};
+        io.base[0] = &bo[0];
+        io.base[1] = &bo[1];
+        mp_unpack_impl(s.mp, 1, reinterpret_cast<const uint32_t *>(plan->h_out + s.off), &plan->exps[i], io, nullptr,
+                       nullptr, shift);
+      } else {
+        const int K = s.form == MPFFT_FORM_DOUBLE ? 1 : tier_words(family_tier(form_family(s.form)));
+        const bool fl = s.form == MPFFT_FORM_FLOAT_FLOAT;
+        for (unsigned long q = 0; q < s.n; ++q)
+          for (int c = 0; c < 2; ++c)
+            words_to_mpfr(plan->h_out + s.off, (size_t)c * K * s.n + q, s.n, K, fl, shift, acc, (c ? outi : outr)[i][q]);
+      }
+    }
+    mpfr_clear(acc);
+  });
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_batch_autotune(mpfft_batch_plan *plan, int save) {
+  if (!plan) return set_err(MPFFT_EINVAL, "NULL argument");
+  std::lock_guard<std::mutex> g(plan->mu);
+  auto table = tune_load();
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  for (size_t q = 0; q < plan->queues.size(); ++q) {
+    auto &Q = plan->queues[q];
+    std::vector<std::pair<int, int>> cand;
+    for (int th : {128, 256}) {
+      if (Q.family == kQueueLimbs) {
+        cand.emplace_back(th, 0);
+        continue;
+      }
+      const int top = family_default_sub(Q.family);
+      for (int sub : {top, top / 2, top / 4}) cand.emplace_back(th, sub);
+    }
+    float best = 1e30f;
+    std::pair<int, int> pick(Q.threads, Q.sub);
+    for (auto &c : cand) {
+      Q.threads = c.first;
+      Q.sub = c.second;
+      if (int e = batch_build_queue(plan, (int)q)) return e;
+      CUDA_TRY(cudaMemcpy(plan->d_tabs, plan->tabs.data(), plan->tabs.size() * sizeof(QueueTables),
+                          cudaMemcpyHostToDevice));
+      float ms = 0, tot = 0;
+      for (int rep = 0; rep < 4; ++rep) {
+        CUDA_TRY(cudaMemsetAsync(plan->d_heads + q, 0, sizeof(int), plan->stream));
+        CUDA_TRY(cudaEventRecord(e0, plan->stream));
+        CUDA_TRY(queue_launch(Q.family, Q.L, Q.d_items, (int)Q.sigs.size(), plan->d_heads + q, Q.ctas, Q.threads, 1.0,
+                              plan->stream));
+        CUDA_TRY(cudaEventRecord(e1, plan->stream));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep) tot += ms;  // the first run warms the caches
+      }
+      if (tot < best) {
+        best = tot;
+        pick = c;
+      }
+    }
+    Q.threads = pick.first;
+    Q.sub = pick.second;
+    if (int e = batch_build_queue(plan, (int)q)) return e;
+    table[tune_key(plan, (int)q)] = pick;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (int e = batch_capture(plan)) return e;
+  if (save) tune_save(table);
+  return set_err(MPFFT_OK, "");
+}
+
+MPFFT_API int mpfft_batch_queue_info(const mpfft_batch_plan *plan, int q, int *family, int *limbs, int *threads,
+                                     int *sub, int *signals) {
+  if (!plan || !family || !limbs || !threads || !sub || !signals) return set_err(MPFFT_EINVAL, "NULL argument");
+  if (q < 0) return (int)plan->queues.size();
+  if ((size_t)q >= plan->queues.size()) return set_err(MPFFT_EINVAL, "queue %d out of range", q);
+  const auto &Q = plan->queues[q];
+  *family = Q.family;
+  *limbs = Q.L;
+  *threads = Q.threads;
+  *sub = Q.sub;
+  *signals = (int)Q.sigs.size();
+  return set_err(MPFFT_OK, "");
+}

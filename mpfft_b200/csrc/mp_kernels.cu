@@ -17,6 +17,7 @@
 //   base[((c*L + i)*N + p)*B + b].
 #include <cstdint>
 
+#include "mp_bfly.cuh"
 #include "mp_limbs.cuh"
 #include "mpfft_internal.h"
 
@@ -32,71 +33,7 @@ __global__ void __launch_bounds__(256) mp_leaf_kernel(const uint32_t *__restrict
                                                        int nleaves) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)nleaves * B) return;
-  const int b = (int)(t % B);
-  const MpLeaf lf = leaves[t / B];
-  const size_t plane = (size_t)N * B;   // distance between limb planes
-  const size_t cim = (size_t)L * plane; // real -> imaginary component
-  // element j of the leaf's subsequence: index (sn + j*s), j=0 wrapped to sn+N
-  int idx[4];
-#pragma unroll
-  for (int j = 0; j < 4; ++j) idx[j] = (j == 0 && lf.sn < 0) ? lf.sn + N : lf.sn + j * lf.s;
-  const uint32_t *x[4];
-#pragma unroll
-  for (int j = 0; j < 4; ++j) x[j] = in + (size_t)(j < lf.n ? idx[j] : 0) * B + b;
-  uint32_t *y = out + (size_t)lf.out * B + b;
-  const size_t yB = B;
-
-  if (lf.n == 4) {
-    // X0 = x0+x2 + (x1+x3)      X2 = x0+x2 - (x1+x3)
-    // X1 = x0-x2 - i(x1-x3)     X3 = x0-x2 + i(x1-x3)
-    int64_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-    for (int i = 0; i < L; ++i) {
-      const size_t o = i * plane;
-      int64_t r[4], m[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const uint32_t vr = x[j][o], vi = x[j][o + cim];
-        r[j] = (i == L - 1) ? (int64_t)(int32_t)vr : (int64_t)vr;
-        m[j] = (i == L - 1) ? (int64_t)(int32_t)vi : (int64_t)vi;
-      }
-      const int64_t er = r[0] + r[2], fr = r[0] - r[2], gr = r[1] + r[3], hr = r[1] - r[3];
-      const int64_t ei = m[0] + m[2], fi = m[0] - m[2], gi = m[1] + m[3], hi = m[1] - m[3];
-      const int64_t v[8] = {c[0] + er + gr, c[1] + fr + hi, c[2] + er - gr, c[3] + fr - hi,
-                            c[4] + ei + gi, c[5] + fi - hr, c[6] + ei - gi, c[7] + fi + hr};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        y[o + q * yB] = (uint32_t)v[q];
-        y[o + cim + q * yB] = (uint32_t)v[4 + q];
-      }
-#pragma unroll
-      for (int q = 0; q < 8; ++q) c[q] = v[q] >> 32;
-    }
-  } else if (lf.n == 2) {
-    int64_t c[4] = {0, 0, 0, 0};
-#pragma unroll
-    for (int i = 0; i < L; ++i) {
-      const size_t o = i * plane;
-      int64_t r0 = x[0][o], r1 = x[1][o], i0 = x[0][o + cim], i1 = x[1][o + cim];
-      if (i == L - 1) {
-        r0 = (int32_t)r0; r1 = (int32_t)r1; i0 = (int32_t)i0; i1 = (int32_t)i1;
-      }
-      const int64_t v[4] = {c[0] + r0 + r1, c[1] + r0 - r1, c[2] + i0 + i1, c[3] + i0 - i1};
-      y[o] = (uint32_t)v[0];
-      y[o + yB] = (uint32_t)v[1];
-      y[o + cim] = (uint32_t)v[2];
-      y[o + cim + yB] = (uint32_t)v[3];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) c[q] = v[q] >> 32;
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < L; ++i) {
-      const size_t o = i * plane;
-      y[o] = x[0][o];
-      y[o + cim] = x[0][o + cim];
-    }
-  }
+  mp_leaf_one<L>(in, out, N, B, (int)(t % B), leaves[t / B]);
 }
 
 // The same leaves for launches too small to fill the GPU: one thread per
@@ -174,37 +111,6 @@ __global__ void __launch_bounds__(128) mp_leaf_small_kernel(const uint32_t *__re
 }
 
 // ---------------------------------------------------------------------------
-// L-shaped combine of one butterfly (reference :238-252), streamed limb by
-// limb: a1 = m1 + m2, a2 = m1 - m2, then U0 +/- a1 and U1 -/+ i a2, twelve
-// independent modular carry chains.  m1 = Z+ w^k and m2 = Z- w^-k sit in the
-// Z+ / Z- slots; when `swapped`, each slot holds (imag, real) instead of
-// (real, imag) -- the twiddle stage writes them that way to stay in place.
-// ---------------------------------------------------------------------------
-template <int L>
-__device__ __forceinline__ void combine(uint32_t *u0, uint32_t *u1, uint32_t *zp, uint32_t *zm, size_t plane,
-                                        size_t cim, bool swapped) {
-  const size_t sre = swapped ? cim : 0, sim = swapped ? 0 : cim;
-  // carry-in of each chain: 0 for additions, 1 for subtractions (a - b = a + ~b + 1)
-  uint32_t ca1r = 0, ca1i = 0, ca2r = 1, ca2i = 1;
-  uint32_t c0r = 0, c2r = 1, c1r = 0, c3r = 1, c0i = 0, c2i = 1, c1i = 1, c3i = 0;
-#pragma unroll
-  for (int i = 0; i < L; ++i, u0 += plane, u1 += plane, zp += plane, zm += plane) {
-    const uint32_t U0r = u0[0], U0i = u0[cim], U1r = u1[0], U1i = u1[cim];
-    const uint32_t m1r = zp[sre], m1i = zp[sim], m2r = zm[sre], m2i = zm[sim];
-    const uint32_t a1r = addc(m1r, m2r, ca1r), a1i = addc(m1i, m2i, ca1i);
-    const uint32_t a2r = addc(m1r, ~m2r, ca2r), a2i = addc(m1i, ~m2i, ca2i);
-    u0[0] = addc(U0r, a1r, c0r);
-    zp[0] = addc(U0r, ~a1r, c2r);
-    u1[0] = addc(U1r, a2i, c1r);
-    zm[0] = addc(U1r, ~a2i, c3r);
-    u0[cim] = addc(U0i, a1i, c0i);
-    zp[cim] = addc(U0i, ~a1i, c2i);
-    u1[cim] = addc(U1i, ~a2r, c1i);
-    zm[cim] = addc(U1i, a2r, c3i);
-  }
-}
-
-// ---------------------------------------------------------------------------
 // one launch = every butterfly of every node of size n
 // ---------------------------------------------------------------------------
 //
@@ -258,93 +164,18 @@ __global__ void __launch_bounds__(128, level_min_blocks<L>()) mp_level_kernel(ui
   const long long r = t / B;
   const int k = (int)(r % q);
   const int off = node_off[r / q];
-  const size_t plane = (size_t)N * B;
-  const size_t cim = (size_t)L * plane;
-  uint32_t *u0 = y + (size_t)(off + k) * B + b;
-  uint32_t *u1 = u0 + (size_t)q * B;
-  uint32_t *zp = u0 + (size_t)2 * q * B;
-  uint32_t *zm = u0 + (size_t)3 * q * B;
-
-  if (k == 0) {
-    combine<L>(u0, u1, zp, zm, plane, cim, false);
-    return;
-  }
-  const size_t tplane = (size_t)(N >> 2) * tws;  // twiddle limb-plane stride
-  const int kn = k * (N / n) * tws;
-  const uint32_t *wr = tw + kn;                           // cos
-  const uint32_t *ws = tw + (size_t)L * tplane + kn;      // cos + sin
-  const uint32_t *wd = tw + (size_t)2 * L * tplane + kn;  // |cos - sin|
-  const bool special = (2 * k == q);
-  const bool dn = special ? false : (dneg[kn] != 0);
-  constexpr int Lp = (L + 3) & ~3;  // packed twiddle stride: 16-byte aligned rows
+  constexpr int Lp = (L + 3) & ~3;
   __shared__ __align__(16) uint32_t Tw[kPackedTw ? 3 * Lp : 4];
-  if (kPackedTw) {  // cos, cos+sin, |cos-sin| of this CTA's k
+  if (kPackedTw && k != 0) {  // cos, cos+sin, |cos-sin| of this CTA's k (every thread of the CTA has it)
+    const size_t tplane = (size_t)(N >> 2) * tws;
+    const int kn = k * (N / n) * tws;
     for (int e = threadIdx.x; e < 3 * L; e += blockDim.x) {
       const int sel = e / L, j = e - sel * L;
       Tw[sel * Lp + j] = tw[(size_t)(sel * L + j) * tplane + kn];
     }
     __syncthreads();
   }
-  uint32_t *P = Ps + threadIdx.x;
-  const size_t ps = blockDim.x;
-  uint32_t X[L];
-#pragma unroll 1
-  for (int st_ = 0; st_ < 6; ++st_) {
-    const int side = st_ >= 3;
-    const int step = st_ - 3 * side;
-    uint32_t *zr = side ? zm : zp;
-    uint32_t *zi = zr + cim;
-    const uint32_t *pa = zr, *pb = nullptr, *w = wr;
-    int wsel = 0;  // packed twiddle row: 0 cos, 1 cos+sin, 2 |cos-sin|
-    bool sub = false, negx = false, mul = true;
-    int sp = 0;
-    uint32_t *dst = nullptr;  // null: the product becomes P
-    if (step == 0) {
-      pb = zi;
-      sub = side;
-    } else if (!special) {
-      if (step == 1) {
-        pa = zi;
-        w = wd;
-        wsel = 2;
-        negx = dn ^ (side == 0);
-        sp = 1;
-        dst = zi;
-      } else {
-        w = ws;
-        wsel = 1;
-        negx = (side == 0);
-        sp = side ? -1 : 1;
-        dst = zr;
-      }
-    } else {
-      if (step == 1) {
-        pa = side ? zr : zi;
-        pb = side ? zi : zr;
-        sub = !side;
-        dst = zr;
-      } else {
-        mul = false;
-        sp = 1;
-        dst = zi;
-      }
-    }
-    if (mul) {
-      ld_addsub<L>(X, pa, pb, plane, sub);
-      if (kPackedTw) mul_tw<L, true>(X, Tw + wsel * Lp, 0);
-      else mul_tw<L>(X, w, tplane);
-    } else {
-#pragma unroll
-      for (int i = 0; i < L; ++i) X[i] = 0;
-    }
-    if (!dst) {
-      st<L>(P, ps, X);
-    } else {
-      combine_p<L>(X, P, ps, negx, sp);
-      st<L>(dst, plane, X);
-    }
-  }
-  combine<L>(u0, u1, zp, zm, plane, cim, true);
+  mp_bfly_one<L, kPackedTw>(y, N, B, b, n, off, k, tw, dneg, tws, Ps + threadIdx.x, blockDim.x, Tw);
 }
 
 // ---------------------------------------------------------------------------

@@ -603,6 +603,75 @@ __global__ void __launch_bounds__(kTcRows, 1)
 }
 
 // ---------------------------------------------------------------------------
+// the int8 tensor-core rate (the roofline denominator of the products above)
+// ---------------------------------------------------------------------------
+//
+// Thread 0 of each CTA issues `count` MMAs of M=128, N=256, K=32 unsigned
+// bytes into one 256-column tensor-memory accumulator (operands: zeroed
+// shared-memory tiles, no-swizzle K-major as above), commits them to an
+// mbarrier and waits for it (bounded); MACs = count * 128*256*32 per CTA.
+static cudaError_t tc_prepare(const void *fn, uint32_t bytes, int **err);
+constexpr uint32_t kTcPeakIdesc = (2u << 4) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kTcPeakSmem = 80u * 1024u;  // keeps a third CTA off an SM (2 x 256 columns)
+
+__global__ void __launch_bounds__(128, 1) mp_tc_peak_kernel(int count, int *err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  // A: 128 rows x 32 bytes at 0, B: 256 rows x 32 bytes at 4096; slot and barrier after
+  for (int i = threadIdx.x; i < (4096 + 8192) / 16; i += blockDim.x) reinterpret_cast<uint4 *>(sm)[i] = make_uint4(0, 0, 0, 0);
+  const uint32_t base = smem_addr(sm), bar = base + 12288, slot = base + 12304;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(256u) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(sm + 12304);
+  if (threadIdx.x == 0) {
+    const uint64_t da = tc_desc(base, 128u, 256u), db = tc_desc(base + 4096u, 128u, 256u);
+    for (int i = 0; i < count; ++i) tc_mma(tmem, da, db, kTcPeakIdesc, i > 0 ? 1u : 0u);
+    tc_commit(bar);
+    if (!mbar_wait(bar, 0, kTcDrainNs)) atomicCAS(err, 0, 2);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u) : "memory");
+  }
+}
+
+cudaError_t mp_tc_int8_rate(double *macs_per_s) {
+  int *err = nullptr;
+  cudaError_t e = tc_prepare((const void *)mp_tc_peak_kernel, kTcPeakSmem, &err);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int ctas = 2 * sms, count = 16384;
+  mp_tc_peak_kernel<<<ctas, 128, kTcPeakSmem>>>(256, err);  // warm-up
+  cudaEventRecord(e0);
+  mp_tc_peak_kernel<<<ctas, 128, kTcPeakSmem>>>(count, err);
+  cudaEventRecord(e1);
+  e = cudaEventSynchronize(e1);
+  float ms = 0;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) *macs_per_s = (double)ctas * count * 128.0 * 256.0 * 32.0 / (ms * 1e-3);
+  return e;
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 

@@ -164,6 +164,8 @@ cudaError_t mp_tc_run_levels(int L, const MpDeviceTables &T, uint32_t *out, int 
 cudaError_t mp_tc_mul(int L, int B, const uint32_t *x, const uint32_t *w, uint32_t *out, cudaStream_t s);
 // reads and clears the device-side error flag of the tensor-core kernels
 cudaError_t mp_tc_take_error(int *code);
+// measured int8 tensor-core rate (multiply-adds per second, kind::i8 MMAs)
+cudaError_t mp_tc_int8_rate(double *macs_per_s);
 // limit of the tensor-core kernels' waits on their own MMAs (ns); tests only
 cudaError_t mp_tc_set_wait_limit(unsigned long long ns);
 size_t mp_tc_smem_bytes(int L);
@@ -206,6 +208,39 @@ int tier_sub_max(int tier);
 // split step of the FP64 real transforms (n = 2M real points), d_kernels.cu
 cudaError_t d_real_split(bool forward, const double *in, double *out, int M, int B, const double *wc,
                          const double *ws, double scale, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// persistent work-queue kernels (queue_kernels.cu)
+// ---------------------------------------------------------------------------
+// What one CTA needs to transform one signal of a given form and length:
+// limb forms use the breadth-first schedule and twiddles of an N-point mp
+// plan (a single signal: limb planes [c][i][p]); floating forms use the
+// sub-transform roots, schedules, upper levels and twiddles of an N-point
+// FP64 / compensated-tier plan (layout [c][h][p]).
+struct QueueTables {
+  int N = 0;
+  TreeTables tree;                 // limb forms
+  const uint32_t *tw = nullptr;    // limb forms: [3][L][N/4]
+  const uint8_t *dneg = nullptr;
+  DDeviceTables ft;                // floating forms
+};
+// one signal of a queue: its input and output in the form's device layout
+struct QueueItem {
+  const void *in;
+  void *out;
+  const QueueTables *tab;
+};
+// Queue families: limb forms (one kernel per limb count), FP64, and the
+// compensated tiers.  A launch runs `ctas` persistent CTAs of `threads`
+// threads that pop items[0 .. nitems) through *head (an atomic counter the
+// caller zeroes before the launch) until the queue is empty; no CTA ever
+// waits for another.
+enum { kQueueLimbs = 0, kQueueDouble = 1, kQueueTierDD = 2, kQueueTierQD = 3, kQueueTierFF = 4 };
+cudaError_t queue_launch(int family, int L, const QueueItem *items, int nitems, int *head, int ctas, int threads,
+                         double scale, cudaStream_t s);
+// largest resident CTAs per SM of a family's kernel at `threads` threads
+int queue_ctas_per_sm(int family, int L, int threads);
+cudaError_t queue_prepare(int family, int L);  // kernel attributes, before any stream capture
 
 // Import -> transform -> export of device-resident MPFR fields with all
 // working storage in a file-scope device array (static_scratch.cu).  Returns an
