@@ -52,6 +52,8 @@ def parse_args():
     ap.add_argument("--batch", type=int, default=2048, help="signals per GPU per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the extra keys (other configurations, tiers, uneven batch, host roofline)")
     ap.add_argument("--dropin", action="store_true",
                     help="instead of the contract line: latency of one mp_sr24_cp_fft call (one signal of --n points "
                          "at --prec bits, host mpfr_t arrays) next to the reference's serial and OpenMP-4 code")
@@ -299,6 +301,288 @@ def dropin_fp64(args):
                       "speedup_vs_serial": (ser / us) if ser else None}))
 
 
+# ---------------------------------------------------------------------------
+# accuracy of every signal of the step (after timing, on the host cores)
+# ---------------------------------------------------------------------------
+
+def worst_accuracy(n, p, B, xr, xi, yr, yi):
+    """Normwise error of every one of the B GPU outputs against the
+    reference's transform at 2P bits (lab/serial/mp/serial_mp_fft3.c restated
+    by the oracle), and the reference's own error at P on the same inputs; on
+    all host cores (the oracle's C calls release the interpreter lock)."""
+    import concurrent.futures as cf
+
+    from oracle import oracle as O
+
+    L = O.lib()
+    local = threading.local()
+
+    def one(b):
+        if not hasattr(local, "fft"):
+            local.fft = (O.MpFFT(n, 2 * p), O.MpFFT(n, p))
+        def cut(a):  # signal b of a batch of mpfr_t arrays
+            t = O.MpArray(n, p)
+            L.orc_mp_copy(t.ptr, a.ptr + b * n * 32, n)
+            return t
+
+        sr, si, gr, gi = cut(xr), cut(xi), cut(yr), cut(yi)
+        wr, wi = O.mp_pair(n, 2 * p)
+        local.fft[0](sr, si, wr, wi)
+        rr, ri = O.mp_pair(n, p)
+        local.fft[1](sr, si, rr, ri)
+        return O.mp_errors(gr, gi, wr, wi)["log2_rel"], O.mp_errors(rr, ri, wr, wi)["log2_rel"]
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        res = list(ex.map(one, range(B)))
+    worst = max(range(B), key=lambda b: res[b][0])
+    bound = O.mp_bound_log2(n, p)
+    return {"worst_gpu_log2_rel_err": res[worst][0], "worst_signal": worst,
+            "reference_log2_rel_err_at_worst": res[worst][1],
+            "worst_reference_log2_rel_err": max(r[1] for r in res),
+            "signals_checked": B, "signals_over_bound": sum(r[0] > bound for r in res),
+            "signals_worse_than_reference": sum(r[0] > r[1] + 0.5 for r in res),
+            "accuracy_oracle": f"reference transform at {2 * p} bits, all {B} signals "
+                               f"({time.perf_counter() - t0:.1f} s on {os.cpu_count()} host threads)"}
+
+
+# ---------------------------------------------------------------------------
+# extra keys: the other configurations, measured in the same run
+# ---------------------------------------------------------------------------
+
+def _cudart():
+    """The CUDA runtime (plain copies into the uneven batch's device arenas)."""
+    import ctypes as C
+    import glob
+
+    try:
+        return C.CDLL("libcudart.so.12")
+    except OSError:
+        import torch
+
+        d = os.path.join(os.path.dirname(torch.__file__), "..", "nvidia", "cuda_runtime", "lib")
+        return C.CDLL(sorted(glob.glob(os.path.join(d, "libcudart.so*")))[0])
+
+
+def _time_device(fn, reps):
+    """ms per call of fn() on the current stream, CUDA events, after 3 warm-up calls."""
+    import torch
+
+    for _ in range(3):
+        fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def host_bandwidth():
+    """Host memory copy bandwidth over all cores (read + write bytes per
+    second): the denominator of the end-to-end host roofline."""
+    import concurrent.futures as cf
+
+    import numpy as np
+
+    nbytes = 1 << 30
+    a = np.ones(nbytes // 8)
+    b = np.empty_like(a)
+    nt = os.cpu_count() or 1
+    parts = np.array_split(np.arange(a.size), nt)
+    sl = [slice(int(q[0]), int(q[-1]) + 1) for q in parts if q.size]
+
+    def cp(s):
+        np.copyto(b[s], a[s])
+
+    with cf.ThreadPoolExecutor(max_workers=nt) as ex:
+        list(ex.map(cp, sl))
+        best = 1e30
+        for _ in range(3):
+            t0 = time.perf_counter()
+            list(ex.map(cp, sl))
+            best = min(best, time.perf_counter() - t0)
+    return 2 * nbytes / best
+
+
+def measure_extras(args, e2e_fft_s, n, p):
+    import numpy as np
+    import torch
+
+    import mpfft_b200 as M
+    from mpfft_b200 import mparray
+    from mpfft_b200.mparray import synthetic_planes
+
+    out = {}
+    st = torch.cuda.current_stream().cuda_stream
+
+    def guard(key, fn):
+        try:
+            out[key] = fn()
+        except Exception as e:  # recorded, not fatal: the contract line stands on its own
+            out[key] = {"error": f"{type(e).__name__}: {e}"}
+
+    # end-to-end host roofline: host memory traffic per transform / measured bandwidth
+    def host_roofline():
+        nl = (p + 63) // 64
+        per_in = 32 + 8 * nl + (8 * nl + 9)            # mpfr_t struct, significand, staging write
+        per_out = (8 * nl + 9) + 32 + 2 * 8 * nl + 32  # staging read, struct, significand RFO + write, struct write
+        per_fft = 2 * n * (per_in + per_out)
+        bw = host_bandwidth()
+        return {"bytes_per_fft": per_fft, "bytes_per_component": per_in + per_out,
+                "achieved_GBs": e2e_fft_s * per_fft / 1e9, "host_copy_GBs": bw / 1e9,
+                "frac": e2e_fft_s * per_fft / bw,
+                "note": "host memory bytes the mpfr_t gather/scatter must move per transform (in + out), "
+                        "against a multi-threaded host copy; DMA traffic to pinned staging not counted"}
+
+    guard("e2e_host_roofline", host_roofline)
+
+    # configuration 1: one signal per drop-in call, N=1024, P=256, host mpfr_t arrays
+    def dropin():
+        nn, pp = 1024, 256
+        xr, xi = mparray.MpfrArray(nn, pp), mparray.MpfrArray(nn, pp)
+        mparray.fill_uniform(xr, xi, SEED)
+        yr, yi = mparray.MpfrArray(nn, pp), mparray.MpfrArray(nn, pp)
+        for _ in range(20):
+            M.mp_sr24_cp_fft(nn, 1, 0, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
+        reps = 200
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            M.mp_sr24_cp_fft(nn, 1, 0, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
+        us = (time.perf_counter() - t0) / reps * 1e6
+        r = {"workload": "mp_sr24_cp_fft, one signal per call, N=1024, P=256", "us_per_call": us}
+        from oracle import oracle as O
+
+        if O.ref_available("mp_ser"):
+            ser = _ref_worker("mp_ser", nn, pp, 200, SEED) / 200 / 1e3
+            r.update({"reference_serial_us": ser, "speedup": ser / us})
+        return r
+
+    guard("config1_dropin", dropin)
+
+    # configuration 2: FP64 and double-double, 4096 signals x N=4096, and one FP64 signal of 2^20
+    def fp64_dd():
+        r = {}
+        nn, bb = 4096, 4096
+        g = torch.Generator(device="cuda").manual_seed(1)
+        x = torch.rand((2, bb, nn), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        y = torch.empty_like(x)
+        pl = M.DPlan(nn)
+        ms = _time_device(lambda: pl.execute_device(bb, x.data_ptr(), y.data_ptr(), stream=st), 10)
+        r["fp64_4096x4096"] = {"fft_per_s": bb / ms * 1e3, "ms": ms, "in_out_GBs": 2 * x.numel() * 8 / ms / 1e6}
+        xd = torch.stack((x[0], x[0] * 2.0 ** -60, x[1], x[1] * 2.0 ** -60)).contiguous()
+        yd = torch.empty_like(xd)
+        dd = M.DDPlan(nn)
+        ms = _time_device(lambda: dd.execute_device(bb, xd.data_ptr(), yd.data_ptr(), stream=st), 5)
+        r["dd_4096x4096"] = {"fft_per_s": bb / ms * 1e3, "ms": ms, "in_out_GBs": 2 * xd.numel() * 8 / ms / 1e6}
+        del x, y, xd, yd
+        big = 1 << 20
+        x1 = torch.rand((2, 1, big), dtype=torch.float64, device="cuda", generator=g)
+        y1 = torch.empty_like(x1)
+        p1 = M.DPlan(big)
+        r["fp64_single_2^20_us"] = _time_device(lambda: p1.execute_device(1, x1.data_ptr(), y1.data_ptr(), stream=st),
+                                                20) * 1e3
+        return r
+
+    guard("config2_fp64_dd", fp64_dd)
+
+    # configuration 3: N=1024, batch 256, P = 64 .. 8192; tensor-core products from 35 limbs
+    def sweep():
+        r = {}
+        tc = M.tc_int8_rate()
+        imad = max(M.imad_rate(False) / 2, M.imad_rate(True))
+        r["int8_tensor_macs_per_s"] = tc
+        r["int_product_peak_per_s"] = imad
+        for pp in (64, 128, 256, 512, 1024, 2048, 4096, 8192):
+            nn, bb = 1024, 256
+            pl = M.MpPlan(nn, pp)
+            host = synthetic_planes(nn, pl.limbs, pl.frac_bits, bb, seed=pp)
+            d_in = torch.from_numpy(host.view(np.int32)).cuda()
+            d_out = torch.empty_like(d_in)
+            ms = _time_device(lambda: pl.execute_device(bb, d_in.data_ptr(), d_out.data_ptr(), st), 3)
+            fps = bb / ms * 1e3
+            e = {"limbs": pl.limbs, "form": ["limbs", "tensor"][pl.form()], "fft_per_s": fps}
+            if pl.form() == 1:  # byte products: cmul(N) (P/8)^2 per transform against the measured int8 rate
+                e["tensor_frac"] = 7172 * (pp / 8) ** 2 * fps / tc
+            else:
+                e["int_frac"] = 7172 * ((pp + 31) // 32) ** 2 * fps / imad
+            r[str(pp)] = e
+            del d_in, d_out
+        return r
+
+    guard("config3_sweep", sweep)
+
+    # the compensated tiers at N=4096 x 4096 signals (device resident)
+    def tiers():
+        r = {}
+        nn, bb = 4096, 4096
+        for t in ("ff", "qd"):
+            pl = M.MultiwordPlan(nn, t)
+            dt = torch.float32 if pl.word_bytes == 4 else torch.float64
+            x = (torch.rand((2, pl.words, bb, nn), dtype=torch.float64, device="cuda") * 2 - 1).to(dt)
+            x[:, 1:] *= 2.0 ** -60 if dt == torch.float64 else 2.0 ** -30
+            y = torch.empty_like(x)
+            ms = _time_device(lambda: pl.execute_device(bb, x.data_ptr(), y.data_ptr(), stream=st), 3)
+            r[t] = {"fft_per_s": bb / ms * 1e3, "ms": ms}
+            del x, y
+        return r
+
+    guard("tiers_4096x4096", tiers)
+
+    # configuration 4: 10,000 signals, N log-uniform 2^4..2^16, P from {24, 53, 106, 212, 512, 1024}
+    # (native tiers for the first four), 5 % scaled by 2^+-40 -- one graph launch
+    def uneven():
+        import ctypes as C
+
+        rng = np.random.default_rng(SEED)
+        cnt = 10000
+        ns = [1 << int(v) for v in rng.integers(4, 17, cnt)]
+        ps = [int(v) for v in rng.choice([24, 53, 106, 212, 512, 1024], cnt)]
+        t0 = time.perf_counter()
+        bp = M.BatchPlan(ns, ps, float_tiers="native")
+        t_plan = time.perf_counter() - t0
+        d_in, d_out, nbytes = bp.arenas()
+        rt = _cudart()
+        # inputs: uniform [-1,1) doubles (floats for float-float) in every floating signal,
+        # random limbs with the top limb cleared (|A| < 2^F) in every limb signal; 5 % of the
+        # floating signals scaled by 2^+-40
+        pat_d = (torch.rand(1 << 21, dtype=torch.float64, device="cuda") * 2 - 1)
+        pat_f = pat_d.to(torch.float32)
+        pat_i = torch.randint(-2**31, 2**31 - 1, (1 << 23,), dtype=torch.int32, device="cuda")
+        sc = {40: pat_d * 2.0 ** 40, -40: pat_d * 2.0 ** -40}
+        torch.cuda.synchronize()
+        scales = rng.choice([0, 40, -40], cnt, p=[0.9, 0.05, 0.05])
+        points = 0
+        for i in range(cnt):
+            form, words, off, nb = bp.signal_format(i)
+            points += ns[i]
+            if form == M.FORM_LIMBS:
+                src = pat_i
+            elif form == M.FORM_FLOAT_FLOAT:
+                src = pat_f
+            else:
+                src = sc.get(int(scales[i]), pat_d)
+            rt.cudaMemcpy(C.c_void_p(d_in + off), C.c_void_p(src.data_ptr()), C.c_size_t(nb), 3)
+            if form == M.FORM_LIMBS:  # top limb planes of the real and imaginary parts
+                top = (words - 1) * ns[i] * 4
+                for c in (0, 1):
+                    rt.cudaMemset(C.c_void_p(d_in + off + c * words * ns[i] * 4 + top), 0, C.c_size_t(ns[i] * 4))
+        rt.cudaDeviceSynchronize()
+        ms = _time_device(lambda: bp.execute_device(st), 5)
+        r = {"signals": cnt, "points": points, "plan_s": t_plan, "ms": ms, "signals_per_s": cnt / ms * 1e3,
+             "points_per_s": points / ms * 1e3, "arena_bytes": nbytes, "queues": bp.queues()}
+        bp.autotune(save=False)
+        ms2 = _time_device(lambda: bp.execute_device(st), 5)
+        r.update({"autotuned_ms": ms2, "autotuned_queues": bp.queues()})
+        bp.close()
+        return r
+
+    guard("config4_uneven", uneven)
+    return out
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -424,7 +708,7 @@ def main():
     # ---- end to end through the C ABI with host mpfr_t arrays ----
     yr, yi = mparray.MpfrArray(n * B, p), mparray.MpfrArray(n * B, p)
     plan.execute(B, xr.ptr, xi.ptr, yr.ptr, yi.ptr)  # warm (pinned staging allocated here)
-    e2e_steps = max(2, min(args.steps, 5))
+    e2e_steps = args.steps
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
@@ -434,9 +718,10 @@ def main():
     dt = max_over_ranks(time.perf_counter() - t0, device="cuda")
     e2e = e2e_steps * B * world / dt
 
-    # ---- accuracy of signal 0 against the 2P-bit oracle (CPU baseline leg) ----
+    # ---- accuracy against the oracle (CPU baseline leg, after timing) ----
     acc = {}
     if rank == 0 and world == 1 and not args.no_accuracy:
+        acc.update(worst_accuracy(n, p, B, xr, xi, yr, yi))
         from oracle import oracle as O
 
         gr, gi = O.mp_pair(n, p)
@@ -449,9 +734,13 @@ def main():
         O.mp_dft(sr, si, dr, di)
         rr, ri = O.mp_pair(n, p)
         O.MpFFT(n, p)(sr, si, rr, ri)
-        acc = {"gpu_log2_rel_err": O.mp_errors(gr, gi, dr, di)["log2_rel"],
+        acc.update({"gpu_log2_rel_err": O.mp_errors(gr, gi, dr, di)["log2_rel"],
                "reference_log2_rel_err": O.mp_errors(rr, ri, dr, di)["log2_rel"],
-               "bound_log2": O.mp_bound_log2(n, p), "oracle": f"direct DFT at {2 * p} bits, signal 0"}
+               "bound_log2": O.mp_bound_log2(n, p), "oracle": f"direct DFT at {2 * p} bits, signal 0"})
+
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras = measure_extras(args, e2e, n, p)
 
     if rank != 0:
         if world > 1:
@@ -484,6 +773,8 @@ def main():
         "launch_ms": {"leaf": leaf_ms, "levels": dict(zip([s[0] for s in sched], level_ms))},
         "clocks": clk.summary(),
     }
+    if extras:
+        line["extras"] = extras
     if base:
         line["cpu_baseline"] = {
             "value": statistics.median(base["rates"]), "unit": "FFT/s", "cores": base["procs"], "kind": "reference",

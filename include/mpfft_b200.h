@@ -65,6 +65,9 @@ extern "C" {
 #define MPFFT_PLAN_TENSOR 32u    /* plan creation: tensor-core twiddle products from 8 limbs up */
 #define MPFFT_PLAN_FLOAT_TIERS 64u /* plan creation: run host-array transforms of precisions up to 200 bits on a
                                        compensated floating-point tier (see mpfft_mp_plan_form) */
+#define MPFFT_PLAN_ROW_PRODUCTS 256u /* plan creation: batched limb levels form their twiddle products row by row
+                                         (all accumulator words in registers) instead of column by column;
+                                         bit-identical, kept for comparisons */
 #define MPFFT_PLAN_NATIVE_TIERS 128u /* plan creation: precisions up to 212 bits on the smallest floating word format
                                          holding P bits (float-float 48, FP64 53, double-double 106,
                                          quad-double 212), with that tier's own error */

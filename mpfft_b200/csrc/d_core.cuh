@@ -246,12 +246,12 @@ __device__ __forceinline__ void d_sub_instances(const double *__restrict__ in, d
   // gather: element j of instance g to DIT position perm[j]; 8 elements per
   // thread are loaded before any is stored, so their latencies overlap
   const int total = G_here << lgT;
-  for (int e0 = 0; e0 < total; e0 += 8 * 256) {
+  for (int e0 = 0; e0 < total; e0 += 8 * (int)blockDim.x) {
     double vr[8], vi[8];
     int dst[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      const int e = e0 + u * 256 + (int)threadIdx.x;
+      const int e = e0 + u * (int)blockDim.x + (int)threadIdx.x;
       const int g = e >> lgT, j = e & (Tmax - 1);
       dst[u] = -1;
       if (e < total && (SINGLE || j < T)) {

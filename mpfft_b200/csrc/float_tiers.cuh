@@ -346,12 +346,12 @@ __device__ __forceinline__ void tier_sub_instances(const typename NT::W *__restr
   const size_t out_re = swap_out ? cplane : 0, out_im = swap_out ? 0 : cplane;
   // gather: element j of instance g to DIT position perm[j], 4 elements per thread in flight
   const int total = G_here << lgT;
-  for (int e0 = 0; e0 < total; e0 += 4 * 256) {
+  for (int e0 = 0; e0 < total; e0 += 4 * (int)blockDim.x) {
     V vr[4], vi[4];
     int dst[4], gg[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const int e = e0 + u * 256 + (int)threadIdx.x;
+      const int e = e0 + u * (int)blockDim.x + (int)threadIdx.x;
       const int g = e >> lgT, j = e & (Tmax - 1);
       dst[u] = -1;
       gg[u] = g;

@@ -1899,6 +1899,7 @@ MPFFT_API int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, 
   p->force_host_conversion = (flags & MPFFT_PLAN_HOST_CONVERSION) != 0;
   if (flags & MPFFT_PLAN_NO_TENSOR) p->tabs.tc = 0;
   else if (flags & MPFFT_PLAN_TENSOR) p->tabs.tc = 2;
+  if (flags & MPFFT_PLAN_ROW_PRODUCTS) p->tabs.cols = 0;
   if (!p->host_only && mp_tc_used(p->tabs, p->L)) p->form = MPFFT_FORM_TENSOR;
   if (flags & (MPFFT_PLAN_FLOAT_TIERS | MPFFT_PLAN_NATIVE_TIERS))
     if (int e = mp_plan_attach_float_tier(p.get(), (flags & MPFFT_PLAN_NATIVE_TIERS) != 0)) return e;

@@ -86,6 +86,7 @@ def main():
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--no-tensor", action="store_true", help="large precision: integer-pipe products")
     ap.add_argument("--force-tensor", action="store_true", help="tensor-core products from 8 limbs up")
+    ap.add_argument("--row-products", action="store_true", help="batched limb levels: row-by-row products")
     a = ap.parse_args()
     if a.tier == "fp64":
         run_fp64(a)
@@ -93,7 +94,7 @@ def main():
     if a.tier == "dd":
         run_dd(a)
         return
-    plan = M.MpPlan(a.n, a.prec, tensor="force" if a.force_tensor else not a.no_tensor)
+    plan = M.MpPlan(a.n, a.prec, tensor="force" if a.force_tensor else not a.no_tensor, row_products=a.row_products)
     host = synthetic_planes(a.n, plan.limbs, plan.frac_bits, a.batch)
     d_in = torch.from_numpy(host.view(np.int32)).cuda()
     d_out = torch.empty_like(d_in)

@@ -37,10 +37,11 @@ def test_tensor_core_wait_expiry_reports_error_and_recovers(M, orc):
     M.tc_set_wait_limit(0)
     try:
         code = M.mp_sr24_cp_fft(n, 1, 0, xr.ptr, xi.ptr, yr.ptr, yi.ptr)
+        msg = M.last_error()[1]
     finally:
         M.tc_set_wait_limit(2_000_000_000)
-    assert code == M.ECUDA, M.last_error()
-    assert "tensor-core wait expired" in M.last_error()[1]
+    assert code == M.ECUDA, msg
+    assert "tensor-core wait expired" in msg
     assert np.all(np.isnan(yr.to_double())) and np.all(np.isnan(yi.to_double()))
     # the context is still usable and the next call is correct
     assert M.mp_sr24_cp_fft(n, 1, 0, xr.ptr, xi.ptr, yr.ptr, yi.ptr) == M.OK, M.last_error()

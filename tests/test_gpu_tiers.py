@@ -150,7 +150,7 @@ def test_float_tier_dispatch_meets_mp_contract(M, orc, p, form, n):
 
 def test_float_tier_out_of_window_runs_on_limbs(M, orc):
     O = orc
-    n, p, batch = 64, 100, 2
+    n, p, batch = 64, 90, 2
     xr, xi = O.mp_pair(n * batch, p)
     O.fill_uniform(xr, xi, 3)
     O.lib().orc_mp_scale2(xr.ptr, n, 2000)  # beyond the double-double window
