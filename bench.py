@@ -407,6 +407,42 @@ def host_bandwidth():
     return 2 * nbytes / best
 
 
+def fill_uneven_arena(M, bp, ns, rng):
+    """Synthetic inputs in a batch plan's input arena: uniform [-1,1) doubles
+    (floats for float-float) in every floating signal, 5 % of them scaled by
+    2^+-40, and random limbs with the top limb cleared (|A| < 2^F) in every
+    limb signal.  Returns the number of points."""
+    import ctypes as C
+
+    import torch
+
+    d_in, _, _ = bp.arenas()
+    rt = _cudart()
+    pat_d = torch.rand(1 << 21, dtype=torch.float64, device="cuda") * 2 - 1
+    pat_f = pat_d.to(torch.float32)
+    pat_i = torch.randint(-2**31, 2**31 - 1, (1 << 23,), dtype=torch.int32, device="cuda")
+    sc = {40: pat_d * 2.0 ** 40, -40: pat_d * 2.0 ** -40}
+    torch.cuda.synchronize()
+    scales = rng.choice([0, 40, -40], len(ns), p=[0.9, 0.05, 0.05])
+    points = 0
+    for i, n in enumerate(ns):
+        form, words, off, nb = bp.signal_format(i)
+        points += n
+        if form == M.FORM_LIMBS:
+            src = pat_i
+        elif form == M.FORM_FLOAT_FLOAT:
+            src = pat_f
+        else:
+            src = sc.get(int(scales[i]), pat_d)
+        rt.cudaMemcpy(C.c_void_p(d_in + off), C.c_void_p(src.data_ptr()), C.c_size_t(nb), 3)
+        if form == M.FORM_LIMBS:  # the top limb planes of the real and imaginary parts
+            top = (words - 1) * n * 4
+            for c in (0, 1):
+                rt.cudaMemset(C.c_void_p(d_in + off + c * words * n * 4 + top), 0, C.c_size_t(n * 4))
+    rt.cudaDeviceSynchronize()
+    return points
+
+
 def measure_extras(args, e2e_fft_s, n, p):
     import numpy as np
     import torch
@@ -534,8 +570,6 @@ def measure_extras(args, e2e_fft_s, n, p):
     # configuration 4: 10,000 signals, N log-uniform 2^4..2^16, P from {24, 53, 106, 212, 512, 1024}
     # (native tiers for the first four), 5 % scaled by 2^+-40 -- one graph launch
     def uneven():
-        import ctypes as C
-
         rng = np.random.default_rng(SEED)
         cnt = 10000
         ns = [1 << int(v) for v in rng.integers(4, 17, cnt)]
@@ -543,33 +577,8 @@ def measure_extras(args, e2e_fft_s, n, p):
         t0 = time.perf_counter()
         bp = M.BatchPlan(ns, ps, float_tiers="native")
         t_plan = time.perf_counter() - t0
+        points = fill_uneven_arena(M, bp, ns, rng)
         d_in, d_out, nbytes = bp.arenas()
-        rt = _cudart()
-        # inputs: uniform [-1,1) doubles (floats for float-float) in every floating signal,
-        # random limbs with the top limb cleared (|A| < 2^F) in every limb signal; 5 % of the
-        # floating signals scaled by 2^+-40
-        pat_d = (torch.rand(1 << 21, dtype=torch.float64, device="cuda") * 2 - 1)
-        pat_f = pat_d.to(torch.float32)
-        pat_i = torch.randint(-2**31, 2**31 - 1, (1 << 23,), dtype=torch.int32, device="cuda")
-        sc = {40: pat_d * 2.0 ** 40, -40: pat_d * 2.0 ** -40}
-        torch.cuda.synchronize()
-        scales = rng.choice([0, 40, -40], cnt, p=[0.9, 0.05, 0.05])
-        points = 0
-        for i in range(cnt):
-            form, words, off, nb = bp.signal_format(i)
-            points += ns[i]
-            if form == M.FORM_LIMBS:
-                src = pat_i
-            elif form == M.FORM_FLOAT_FLOAT:
-                src = pat_f
-            else:
-                src = sc.get(int(scales[i]), pat_d)
-            rt.cudaMemcpy(C.c_void_p(d_in + off), C.c_void_p(src.data_ptr()), C.c_size_t(nb), 3)
-            if form == M.FORM_LIMBS:  # top limb planes of the real and imaginary parts
-                top = (words - 1) * ns[i] * 4
-                for c in (0, 1):
-                    rt.cudaMemset(C.c_void_p(d_in + off + c * words * ns[i] * 4 + top), 0, C.c_size_t(ns[i] * 4))
-        rt.cudaDeviceSynchronize()
         ms = _time_device(lambda: bp.execute_device(st), 5)
         r = {"signals": cnt, "points": points, "plan_s": t_plan, "ms": ms, "signals_per_s": cnt / ms * 1e3,
              "points_per_s": points / ms * 1e3, "arena_bytes": nbytes, "queues": bp.queues()}

@@ -65,9 +65,6 @@ extern "C" {
 #define MPFFT_PLAN_TENSOR 32u    /* plan creation: tensor-core twiddle products from 8 limbs up */
 #define MPFFT_PLAN_FLOAT_TIERS 64u /* plan creation: run host-array transforms of precisions up to 200 bits on a
                                        compensated floating-point tier (see mpfft_mp_plan_form) */
-#define MPFFT_PLAN_ROW_PRODUCTS 256u /* plan creation: batched limb levels form their twiddle products row by row
-                                         (all accumulator words in registers) instead of column by column;
-                                         bit-identical, kept for comparisons */
 #define MPFFT_PLAN_NATIVE_TIERS 128u /* plan creation: precisions up to 212 bits on the smallest floating word format
                                          holding P bits (float-float 48, FP64 53, double-double 106,
                                          quad-double 212), with that tier's own error */
@@ -328,7 +325,8 @@ int mpfft_batch_signal_format(const mpfft_batch_plan *plan, unsigned long i, int
 /* device addresses and size of the input and output arenas */
 int mpfft_batch_arenas(const mpfft_batch_plan *plan, void **d_in, void **d_out, size_t *bytes);
 /* One graph launch on `stream`: every signal of the input arena into the
- * output arena (forward, unscaled).  Asynchronous. */
+ * output arena (forward, unscaled).  Asynchronous; executions of one plan
+ * share its arenas, so executions that overlap on the GPU race. */
 int mpfft_batch_execute_device(mpfft_batch_plan *plan, void *stream);
 /* Host mpfr_t arrays, signal i at inr[i][0..n[i]) etc.: converted into the
  * arena on the host (limb signals with one block exponent each, floating

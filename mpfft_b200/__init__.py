@@ -32,7 +32,6 @@ PLAN_NO_TENSOR = 16
 PLAN_TENSOR = 32
 PLAN_FLOAT_TIERS = 64
 PLAN_NATIVE_TIERS = 128
-PLAN_ROW_PRODUCTS = 256
 FORM_LIMBS, FORM_TENSOR, FORM_FLOAT_FLOAT, FORM_DOUBLE, FORM_DOUBLE_DOUBLE, FORM_QUAD_DOUBLE = range(6)
 
 
@@ -203,7 +202,7 @@ class MpPlan:
     """Multiprecision plan for n points at `prec` bits (device limb format)."""
 
     def __init__(self, n: int, prec: int, host_only: bool = False, host_conversion: bool = False,
-                 tensor=True, float_tiers=False, row_products=False):
+                 tensor=True, float_tiers=False):
         """tensor: True (default choice), False (integer pipes only) or
         "force" (tensor-core products from 8 limbs up).  float_tiers: True runs
         precisions a compensated floating-point tier covers within the mp
@@ -212,8 +211,7 @@ class MpPlan:
         h = C.c_void_p()
         flags = ((PLAN_HOST_ONLY if host_only else 0) | (PLAN_HOST_CONVERSION if host_conversion else 0)
                  | (PLAN_TENSOR if tensor == "force" else 0 if tensor else PLAN_NO_TENSOR)
-                 | (PLAN_NATIVE_TIERS if float_tiers == "native" else PLAN_FLOAT_TIERS if float_tiers else 0)
-                 | (PLAN_ROW_PRODUCTS if row_products else 0))
+                 | (PLAN_NATIVE_TIERS if float_tiers == "native" else PLAN_FLOAT_TIERS if float_tiers else 0))
         _check(lib.mpfft_mp_plan_create_flags(C.byref(h), n, prec, flags))
         self.h = h
         self.n, self.prec = n, prec

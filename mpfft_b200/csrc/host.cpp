@@ -1899,7 +1899,6 @@ MPFFT_API int mpfft_mp_plan_create_flags(mpfft_mp_plan **plan, unsigned long n, 
   p->force_host_conversion = (flags & MPFFT_PLAN_HOST_CONVERSION) != 0;
   if (flags & MPFFT_PLAN_NO_TENSOR) p->tabs.tc = 0;
   else if (flags & MPFFT_PLAN_TENSOR) p->tabs.tc = 2;
-  if (flags & MPFFT_PLAN_ROW_PRODUCTS) p->tabs.cols = 0;
   if (!p->host_only && mp_tc_used(p->tabs, p->L)) p->form = MPFFT_FORM_TENSOR;
   if (flags & (MPFFT_PLAN_FLOAT_TIERS | MPFFT_PLAN_NATIVE_TIERS))
     if (int e = mp_plan_attach_float_tier(p.get(), (flags & MPFFT_PLAN_NATIVE_TIERS) != 0)) return e;
@@ -2488,17 +2487,6 @@ static int family_tier(int fam) {
 }
 static int family_default_sub(int fam) { return fam == kQueueDouble ? kDSubMax : tier_sub_max(family_tier(fam)); }
 
-// relative cost of one point-level of each form, for largest-first ordering
-static double form_cost(int fam, int L) {
-  switch (fam) {
-    case kQueueDouble: return 1.0;
-    case kQueueTierFF: return 2.0;
-    case kQueueTierDD: return 8.0;
-    case kQueueTierQD: return 60.0;
-    default: return 0.6 * L * L + 4.0 * L;
-  }
-}
-
 }  // namespace mpfft
 
 struct mpfft_batch_plan {
@@ -2758,7 +2746,6 @@ MPFFT_API int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long cou
       bp->arena += (bp->sig[i].bytes + 255) & ~(size_t)255;
     }
   }
-  (void)form_cost;
   CUDA_TRY(cudaMalloc(&bp->d_tabs, bp->tabs.size() * sizeof(QueueTables)));
   CUDA_TRY(cudaMalloc(&bp->d_heads, bp->queues.size() * sizeof(int)));
   if (dev_alloc((void **)&bp->d_in, bp->arena) != cudaSuccess || dev_alloc((void **)&bp->d_out, bp->arena) != cudaSuccess) {

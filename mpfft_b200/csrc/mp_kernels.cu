@@ -179,126 +179,6 @@ __global__ void __launch_bounds__(128, level_min_blocks<L>()) mp_level_kernel(ui
 }
 
 // ---------------------------------------------------------------------------
-// the same launch with column-by-column products (batches of multiples of 32)
-// ---------------------------------------------------------------------------
-//
-// mp_level_kernel runs each product row by row (mul_tw) with all L+2
-// accumulator words in registers: 128 registers at 33 limbs, four CTAs of 128
-// threads per SM, and the level is bound by global-load latency with few
-// warps to hide it.  When every warp shares one (node, k) -- batches that are
-// a multiple of 32 -- each warp stages its three twiddles in shared memory as
-// mul_tw_cols wants them, and the products run column by column with only the
-// operand and a few words in registers, so twice as many warps fit.  The
-// result limbs stream straight into the merges; operations and operands are
-// those of mp_level_kernel, so the outputs are bit-identical.
-#ifndef MPFFT_COLS_MINB
-#define MPFFT_COLS_MINB 6  // CTAs per SM above 20 limbs
-#endif
-template <int L>
-constexpr int cols_min_blocks() {
-  return L <= 8 ? 12 : (L <= 20 ? 8 : MPFFT_COLS_MINB);
-}
-
-template <int L>
-__global__ void __launch_bounds__(128, cols_min_blocks<L>()) mp_level_cols_kernel(
-    uint32_t *__restrict__ y, int N, int B, int n, const int *__restrict__ node_off, int nnodes,
-    const uint32_t *__restrict__ tw, const uint8_t *__restrict__ dneg, int tws) {
-  constexpr int Lq = cols_stride<L>();
-  __shared__ uint32_t Ps[L * 128];
-  __shared__ __align__(16) uint32_t Wq[4][3][4 * Lq];  // per warp: cos, cos+sin, |cos-sin|, four copies each
-  const int q = n >> 2;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)nnodes * q * B) return;  // whole warps: B is a multiple of 32
-  const int b = (int)(t % B);
-  const long long r = t / B;
-  const int k = (int)(r % q);
-  const int off = node_off[r / q];
-  const size_t plane = (size_t)N * B;
-  const size_t cim = (size_t)L * plane;
-  uint32_t *u0 = y + (size_t)(off + k) * B + b;
-  uint32_t *u1 = u0 + (size_t)q * B;
-  uint32_t *zp = u0 + (size_t)2 * q * B;
-  uint32_t *zm = u0 + (size_t)3 * q * B;
-  if (k == 0) {
-    combine<L>(u0, u1, zp, zm, plane, cim, false);
-    return;
-  }
-  const size_t tplane = (size_t)(N >> 2) * tws;
-  const int kn = k * (N / n) * tws;
-  const bool special = (2 * k == q);
-  const bool dn = special ? false : (dneg[kn] != 0);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t(&W)[3][4 * Lq] = Wq[warp];
-  for (int e = lane; e < 3 * 4 * Lq; e += 32) {  // copy s word u of twiddle sel: w_(L-1-(u-s))
-    const int sel = e / (4 * Lq), rem = e - sel * 4 * Lq, cs = rem / Lq, u = rem - cs * Lq, m = u - cs;
-    W[sel][rem] = (m >= 0 && m < L) ? tw[(size_t)(sel * L + (L - 1 - m)) * tplane + kn] : 0u;
-  }
-  __syncwarp();
-  uint32_t *P = Ps + threadIdx.x;
-  const size_t ps = blockDim.x;
-  uint32_t X[L];
-#pragma unroll 1
-  for (int st_ = 0; st_ < 6; ++st_) {
-    const int side = st_ >= 3;
-    const int step = st_ - 3 * side;
-    uint32_t *zr = side ? zm : zp;
-    uint32_t *zi = zr + cim;
-    const uint32_t *pa = zr, *pb = nullptr;
-    int wsel = 0;  // 0 cos, 1 cos+sin, 2 |cos-sin|
-    bool sub = false, negx = false, mul = true;
-    int sp = 0;
-    uint32_t *dst = nullptr;  // null: the product becomes P
-    if (step == 0) {
-      pb = zi;
-      sub = side;
-    } else if (!special) {
-      if (step == 1) {
-        pa = zi;
-        wsel = 2;
-        negx = dn ^ (side == 0);
-        sp = 1;
-        dst = zi;
-      } else {
-        wsel = 1;
-        negx = (side == 0);
-        sp = side ? -1 : 1;
-        dst = zr;
-      }
-    } else {
-      if (step == 1) {
-        pa = side ? zr : zi;
-        pb = side ? zi : zr;
-        sub = !side;
-        dst = zr;
-      } else {
-        mul = false;
-        sp = 1;
-        dst = zi;
-      }
-    }
-    // the merge of mp_level_kernel (combine_p), streamed limb by limb
-    const uint32_t mx = negx ? 0xffffffffu : 0u;
-    const uint32_t mp = sp < 0 ? 0xffffffffu : 0u;
-    const uint32_t keep = sp != 0 ? 0xffffffffu : 0u;
-    uint32_t cy = (negx ? 1u : 0u) + (sp < 0 ? 1u : 0u);
-    if (mul) {
-      ld_addsub<L>(X, pa, pb, plane, sub);
-      if (!dst) {
-        mul_tw_cols<L>(X, W[wsel], [&](int i, uint32_t v) { P[(size_t)i * ps] = v; });
-      } else {
-        mul_tw_cols<L>(X, W[wsel], [&](int i, uint32_t v) {
-          dst[(size_t)i * plane] = addc(v ^ mx, (P[(size_t)i * ps] & keep) ^ mp, cy);
-        });
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < L; ++i) dst[(size_t)i * plane] = addc(0u ^ mx, (P[(size_t)i * ps] & keep) ^ mp, cy);
-    }
-  }
-  combine<L>(u0, u1, zp, zm, plane, cim, true);
-}
-
-// ---------------------------------------------------------------------------
 // the same launch for batches too small to fill the GPU
 // ---------------------------------------------------------------------------
 //
@@ -473,8 +353,6 @@ __global__ void __launch_bounds__(8 * kSmallBflies) mp_level_small_kernel(uint32
 // threshold loses 17 % at 128 signals, and with 256 signals (65k butterflies
 // per launch) the one-thread-per-butterfly kernel is 1.5x faster.
 constexpr long long kSmallLevelButterflies = 148LL * 128;
-// smallest limb count whose batched levels run mp_level_cols_kernel
-constexpr int kColsMinLimbs = 4;
 
 template <int L>
 static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
@@ -500,9 +378,6 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
     if (total < kSmallLevelButterflies)
       mp_level_small_kernel<L><<<(unsigned)((total + kSmallBflies - 1) / kSmallBflies), 8 * kSmallBflies, 0, s>>>(
           out, T.N, B, n, T.node_off + T.level_start[lv], T.level_count[lv], T.tw, T.dneg, T.tws);
-    else if (T.cols && B % 32 == 0 && L >= kColsMinLimbs)
-      mp_level_cols_kernel<L><<<blocks, lthreads, 0, s>>>(out, T.N, B, n, T.node_off + T.level_start[lv],
-                                                          T.level_count[lv], T.tw, T.dneg, T.tws);
     else if (L <= kPackedTwiddleMaxLimbs && B % lthreads == 0)
       mp_level_kernel<L, (L <= kPackedTwiddleMaxLimbs)><<<blocks, lthreads, 0, s>>>(
           out, T.N, B, n, T.node_off + T.level_start[lv], T.level_count[lv], T.tw, T.dneg, T.tws);

@@ -132,84 +132,3 @@ __device__ __forceinline__ void mul_tw(uint32_t (&x)[L], const uint32_t *w, size
 }
 
 }  // namespace mpfft
-
-namespace mpfft {
-
-// ---------------------------------------------------------------------------
-// the same product, column by column (product scanning)
-// ---------------------------------------------------------------------------
-//
-// mul_tw keeps all L+2 accumulator words of the product in registers next to
-// the L operand limbs.  Here the columns are formed one after another:
-// column c = L-2+a sums x_i * w_(c-i) into a running total whose low word is
-// final (word a) and whose upper two words carry into column c+1.  The
-// integer is the same -- every partial product with i + j >= L-2, 2^30 added
-// in word 1, the twiddle subtracted from word 2 on when x is negative, all
-// modulo 2^(32(L+2)) -- so the rounded result limbs are bit-identical to
-// mul_tw's, with only x and a few words live (about half the registers).
-//
-// The twiddle comes from shared memory reversed (wr[t] = w_(L-1-t)), so that
-// the limbs a column needs are consecutive, in four copies shifted by 0..3
-// words (copy s, word u = wr[u - s], zero outside 0 <= u-s < L) so that every
-// column reads them in aligned 128-bit loads.  Result limb r_i is passed to
-// sink(i, r_i) as soon as words i+1 and i+2 are final, in increasing i.
-template <int L>
-__host__ __device__ constexpr int cols_stride() {
-  return (L + 6 + 3) & ~3;  // words per copy, covering the over-read of the last quad
-}
-
-template <int L, class Sink>
-__device__ __forceinline__ void mul_tw_cols(const uint32_t (&x)[L], const uint32_t *wq, Sink &&sink) {
-  constexpr int Lq = cols_stride<L>();
-  const uint32_t smask = 0u - (x[L - 1] >> 31);
-  uint32_t c0 = 0, c1 = 0;  // carry of the previous column (two words)
-  uint32_t prev = 0;        // word a-1
-#pragma unroll
-  for (int a = 0; a < L + 2; ++a) {
-    const int c = a + L - 2;
-    const int i_lo = c - (L - 1) > 0 ? c - (L - 1) : 0;
-    const int i_hi = c < L - 1 ? c : L - 1;
-    uint32_t t0, t1, t2 = 0;
-    {
-      const uint64_t init = (uint64_t)c0 + (a == 1 ? (1u << 30) : 0u);  // + 2^(32L-2): round to nearest
-      t0 = (uint32_t)init;
-      const uint64_t h = (uint64_t)c1 + (init >> 32);
-      t1 = (uint32_t)h;
-      t2 = (uint32_t)(h >> 32);
-    }
-    if (i_lo <= i_hi) {
-      const int tt = L - 1 - c + i_lo;  // wr index of the column's first limb
-      const int s = (4 - (tt & 3)) & 3;
-      const uint32_t *base = wq + s * Lq + tt + s;  // 16-byte aligned
-#pragma unroll
-      for (int i = i_lo; i <= i_hi; i += 4) {
-        const uint4 v = *reinterpret_cast<const uint4 *>(base + (i - i_lo));
-        const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          if (i + e <= i_hi) {
-            const uint64_t pr = (uint64_t)x[i + e] * wv[e] + t0;
-            t0 = (uint32_t)pr;
-            const uint64_t h = (uint64_t)t1 + (pr >> 32);
-            t1 = (uint32_t)h;
-            t2 += (uint32_t)(h >> 32);
-          }
-        }
-      }
-    }
-    if (a >= 2) {  // signed correction: + ~(w_(a-2) & s) (+1 at a = 2), i.e. - s*w*2^(32L)
-      const uint32_t wj = wq[L + 1 - a];  // copy 0: wr[L+1-a] = w_(a-2)
-      const uint64_t pr = (uint64_t)t0 + (uint32_t)~(wj & smask) + (a == 2 ? 1u : 0u);
-      t0 = (uint32_t)pr;
-      const uint64_t h = (uint64_t)t1 + (pr >> 32);
-      t1 = (uint32_t)h;
-      t2 += (uint32_t)(h >> 32);
-      sink(a - 2, __funnelshift_r(prev, t0, 31));
-    }
-    prev = t0;
-    c0 = t1;
-    c1 = t2;
-  }
-}
-
-}  // namespace mpfft

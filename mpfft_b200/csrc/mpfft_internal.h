@@ -43,7 +43,6 @@ struct MpDeviceTables : TreeTables {
   int tws = 1;  // the table is built for tws*N points (2 for a real transform of 2N points)
   int tc = 1;   // twiddle products on the tensor cores (mp_tc_kernels.cu): 0 never, 1 from
                 // kTcMinLimbs limbs, 2 from kTcForceMinLimbs limbs
-  int cols = 1;  // batched levels (batch a multiple of 32): column-by-column products (1) or row by row (0)
 };
 
 // Schedule of one shared-memory sub-transform of size `size` (FP64 tier):
