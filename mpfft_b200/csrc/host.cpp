@@ -528,7 +528,20 @@ struct mpfft_mp_plan {
   // form the plan reports (MPFFT_FORM_*)
   mpfft_d_plan *fplan = nullptr;
   int form = MPFFT_FORM_LIMBS;
+  // device-layout executions (mpfft_mp_execute_device) replayed from CUDA
+  // graphs, keyed by (batch, input, output); null: that call shape runs its
+  // launches directly.  dev_uses counts the direct runs before a capture.
+  using DevKey = std::tuple<unsigned long, const void *, const void *>;
+  std::map<DevKey, cudaGraphExec_t> dev_graphs;
+  std::map<DevKey, int> dev_uses;
+  void free_dev_graphs() {
+    for (auto &g : dev_graphs)
+      if (g.second) cudaGraphExecDestroy(g.second);
+    dev_graphs.clear();
+    dev_uses.clear();
+  }
   ~mpfft_mp_plan() {
+    free_dev_graphs();
     free_conv();
     d_plan_delete(fplan);
     if (scratch_ev) cudaEventDestroy(scratch_ev);
@@ -2057,6 +2070,36 @@ MPFFT_API int mpfft_mp_execute_c2r(mpfft_mp_plan *plan, unsigned long batch, mpf
   return e;
 }
 
+// One-dimensional integer-pipe plans replay a device-layout call shape
+// (batch, input, output) from a CUDA graph from its second use on: one graph
+// launch instead of one launch per level, which matters for single signals,
+// whose levels are each a few microseconds of device work -- less than the
+// host's cost of issuing them.  Captured on the plan's own stream (the
+// caller's may be the legacy default stream, which cannot be captured) and
+// launched on the caller's.  The first use runs directly, so that nothing is
+// initialised inside a capture; a capture that fails leaves the shape on
+// direct launches.  Called under plan->mu.
+constexpr size_t kDeviceGraphsMax = 16;  // cached call shapes per plan
+
+static cudaGraphExec_t mp_device_graph(mpfft_mp_plan *p, unsigned long batch, const uint32_t *in, uint32_t *out) {
+  const mpfft_mp_plan::DevKey key{batch, in, out};
+  auto it = p->dev_graphs.find(key);
+  if (it != p->dev_graphs.end()) return it->second;
+  if (p->dev_uses.size() >= 4 * kDeviceGraphsMax || p->dev_graphs.size() >= kDeviceGraphsMax) p->free_dev_graphs();
+  if (p->dev_uses[key]++ < 1) return nullptr;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  if (cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+    const cudaError_t e = mp_transform(p, in, out, (int)batch, p->stream, nullptr, nullptr);
+    const cudaError_t ce = cudaStreamEndCapture(p->stream, &g);
+    if (e != cudaSuccess || ce != cudaSuccess || !g || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) ge = nullptr;
+    if (g) cudaGraphDestroy(g);
+  }
+  cudaGetLastError();
+  p->dev_graphs.emplace(key, ge);
+  return ge;
+}
+
 MPFFT_API int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, const uint32_t *d_in,
                                       uint32_t *d_out, void *stream) {
   if (!plan || !d_in || !d_out) return set_err(MPFFT_EINVAL, "NULL argument");
@@ -2073,6 +2116,11 @@ MPFFT_API int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, 
   if (int e = mp_big_reserve(plan, batch, &big)) return e;
   if (int e = mp_tmp_reserve(plan, batch, &tmp)) return e;
   const cudaStream_t st = (cudaStream_t)stream;
+  if (!big && !tmp && plan->rank == 1 && plan->L <= kMaxLimbs && !mp_tc_used(plan->tabs, plan->L))
+    if (cudaGraphExec_t ge = mp_device_graph(plan, batch, d_in, d_out)) {
+      CUDA_TRY(cudaGraphLaunch(ge, st));
+      return set_err(MPFFT_OK, "");
+    }
   if (big || tmp)
     if (int e = scratch_wait(plan, st)) return e;
   CUDA_TRY(mp_transform(plan, d_in, d_out, (int)batch, st, big, tmp));

@@ -18,10 +18,24 @@
 #include <cstdint>
 
 #include "mp_bfly.cuh"
+#include "mp_lanes.cuh"
 #include "mp_limbs.cuh"
 #include "mpfft_internal.h"
 
 namespace mpfft {
+
+// Programmatic dependent launch, for the kernels of launches too small to fill
+// the GPU (one signal: a few microseconds of work each, comparable to the
+// launch latency between them).  Launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization, such a kernel may be
+// scheduled while its predecessor in the stream still runs: it lets its own
+// successor be scheduled at once (pdl_release) and, before its first access
+// to global data that earlier work reads or writes, waits (pdl_wait) until the
+// predecessor grid has completed and its memory is visible.  Plan constants
+// (leaf table, node offsets, twiddles) are read before the wait.  Without the
+// attribute both instructions do nothing.
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // leaves: size-1, size-2 and size-4 DFTs of strided input subsequences
@@ -45,12 +59,14 @@ template <int L>
 __global__ void __launch_bounds__(128) mp_leaf_small_kernel(const uint32_t *__restrict__ in,
                                                             uint32_t *__restrict__ out, int N, int B,
                                                             const MpLeaf *__restrict__ leaves, int nleaves) {
+  pdl_release();
   const long long t = (long long)blockIdx.x * 16 + (threadIdx.x >> 3);
   const int o = threadIdx.x & 7;
   if (t >= (long long)nleaves * B) return;
   const int b = (int)(t % B);
   const MpLeaf lf = leaves[t / B];
   if (o >= 2 * lf.n) return;
+  pdl_wait();
   const size_t plane = (size_t)N * B;
   const size_t cim = (size_t)L * plane;
   // terms of output o: (input element j, imaginary part?, sign)
@@ -293,6 +309,7 @@ __global__ void __launch_bounds__(8 * kSmallBflies) mp_level_small_kernel(uint32
                                                                           int nnodes, const uint32_t *__restrict__ tw,
                                                                           const uint8_t *__restrict__ dneg, int tws) {
   __shared__ uint32_t Qs[kSmallBflies * 6 * L];  // [butterfly][step][limb]
+  pdl_release();
   const int lb = threadIdx.x >> 3, st_ = threadIdx.x & 7;  // steps 0..5; all 8 in the combine
   const int q = n >> 2;
   const long long t = (long long)blockIdx.x * kSmallBflies + lb;
@@ -319,6 +336,7 @@ __global__ void __launch_bounds__(8 * kSmallBflies) mp_level_small_kernel(uint32
       const bool dn = special ? false : (dneg[kn] != 0);
       S = bfly_step(st_, special, dn, zp, zm, cim, tw + kn, tw + (size_t)L * tplane + kn,
                     tw + (size_t)2 * L * tplane + kn);
+      pdl_wait();
       uint32_t X[L];
       if (S.mul) {
         ld_addsub<L>(X, S.pa, S.pb, plane, S.sub);
@@ -330,6 +348,7 @@ __global__ void __launch_bounds__(8 * kSmallBflies) mp_level_small_kernel(uint32
       st<L>(Q, 1, X);
     }
   }
+  pdl_wait();  // (again, for the threads that skipped the product: returns at once)
   __syncthreads();
   if (valid && k != 0 && S.dst) {  // steps 1 and 2: merge with the side's first product
     uint32_t X[L];
@@ -339,6 +358,126 @@ __global__ void __launch_bounds__(8 * kSmallBflies) mp_level_small_kernel(uint32
   }
   __syncthreads();  // the merged Z slots (global) are visible to the CTA
   combine_one<L>(st_, valid, u0, u1, zp, zm, plane, cim, k != 0);
+}
+
+// ---------------------------------------------------------------------------
+// the same launch with each product spread over a warp (fewest butterflies)
+// ---------------------------------------------------------------------------
+//
+// One CTA of eight warps per butterfly, every number's limbs across a warp's
+// lanes (mp_lanes.cuh).  Warps 0..5 run the six twiddle steps of
+// mp_level_small_kernel at once (step = warp), each product as L column sums
+// side by side instead of one thread's ~L^2/2 chained multiply-adds; after a
+// barrier the warps of steps 1, 2, 4, 5 merge with their side's first
+// product, and after a second barrier warp o (0..7) forms output component o
+// of the L-combine (combine_one's table).  The merged products stay in
+// shared memory; every global input a warp needs (its step's operands, its
+// output's U and, without twiddle, the Z slots) is loaded before the first
+// barrier and every output is stored after the second, so the in-place update
+// is safe.  The same sums of the same operands: bit-identical.
+constexpr int kWarpBflyThreads = 256;
+
+template <int L>
+__global__ void __launch_bounds__(kWarpBflyThreads) mp_level_warp_kernel(uint32_t *__restrict__ y, int N, int B,
+                                                                          int n, const int *__restrict__ node_off,
+                                                                          const uint32_t *__restrict__ tw,
+                                                                          const uint8_t *__restrict__ dneg,
+                                                                          int tws) {
+  constexpr bool kTwo = L + 2 > 32;
+  constexpr int Lp = (L + 3) & ~3;
+  constexpr int Wlen = lanes_tw_len<L>();
+  __shared__ __align__(16) uint32_t Xs[6][Lp];  // each step's operand, for broadcast reads
+  __shared__ uint32_t Ws[6][Wlen];              // each step's zero-padded twiddle row
+  __shared__ uint32_t Rs[6][64];                // P (steps 0, 3) and the merged products
+  pdl_release();
+  const int warp = threadIdx.x >> 5;
+  const unsigned lane = lane_index();
+  const int q = n >> 2;
+  const int b = (int)(blockIdx.x % (unsigned)B);
+  const long long r = blockIdx.x / (unsigned)B;
+  const int k = (int)(r % q);
+  const int off = node_off[r / q];
+  const size_t plane = (size_t)N * B;
+  const size_t cim = (size_t)L * plane;
+  uint32_t *u0 = y + (size_t)(off + k) * B + b;
+  uint32_t *u1 = u0 + (size_t)q * B;
+  uint32_t *zp = u0 + (size_t)2 * q * B;
+  uint32_t *zm = u0 + (size_t)3 * q * B;
+
+  // output component o = warp: dst = U -/+ (mA +/- mB)
+  const int o = warp;
+  const bool im_in = (o >= 2 && o <= 5);
+  const bool inner_sub = (o == 2 || o == 3 || o == 6 || o == 7);
+  const bool outer_sub = (o == 1 || o == 3 || o == 5 || o == 6);
+  const uint32_t *U = ((o <= 1 || o == 4 || o == 5) ? u0 : u1) + (o >= 4 ? cim : 0);
+  uint32_t *dst = o == 0 ? u0 : o == 1 ? zp : o == 2 ? u1 : o == 3 ? zm : o == 4 ? u0 + cim
+                : o == 5 ? zp + cim : o == 6 ? u1 + cim : zm + cim;
+  BflyStep S{};
+  uint32_t Xa = 0, Xb = 0, Wa = 0, Wb = 0;
+  const bool special = (2 * k == q);
+  if (k != 0 && warp < 6) {  // the step and its twiddle row (plan constants)
+    const size_t tplane = (size_t)(N >> 2) * tws;
+    const int kn = k * (N / n) * tws;
+    const bool dn = special ? false : (dneg[kn] != 0);
+    S = bfly_step(warp, special, dn, zp, zm, cim, tw + kn, tw + (size_t)L * tplane + kn,
+                  tw + (size_t)2 * L * tplane + kn);
+    if (S.mul) lanes_ld<L, kTwo>(Wa, Wb, S.w, tplane);
+  }
+  pdl_wait();
+  uint32_t Ua, Ub, Aa = 0, Ab = 0, Ba = 0, Bb = 0;
+  lanes_ld<L, kTwo>(Ua, Ub, U, plane);
+  if (k == 0) {  // no twiddle: the Z slots are the products, unswapped
+    lanes_ld<L, kTwo>(Aa, Ab, zp + (im_in ? cim : 0), plane);
+    lanes_ld<L, kTwo>(Ba, Bb, zm + (im_in ? cim : 0), plane);
+  } else if (warp < 6) {
+    if (S.mul) {
+      uint32_t Pa = 0, Pb = 0;
+      lanes_ld<L, kTwo>(Xa, Xb, S.pa, plane);
+      if (S.pb) lanes_ld<L, kTwo>(Pa, Pb, S.pb, plane);
+      uint32_t *W = Ws[warp];  // W[j + L-1] = w_j, zeros around
+      for (int e = (int)lane; e < Wlen; e += 32)
+        if (e < L - 1 || e >= 2 * L - 1) W[e] = 0u;
+      if (lane < L) W[lane + L - 1] = Wa;
+      if (kTwo && lane + 32 < L) W[lane + 32 + L - 1] = Wb;
+      if (S.pb) {
+        const uint32_t m = S.sub ? ~0u : 0u;
+        lanes_add<kTwo>(Xa, Xb, Pa ^ m, Pb ^ m, S.sub ? 1u : 0u);
+      }
+      if (lane < L) Xs[warp][lane] = Xa;
+      if (kTwo && lane + 32 < L) Xs[warp][lane + 32] = Xb;
+      __syncwarp();
+      lanes_mul_tw<L>(Xa, Xb, Xs[warp], W);
+    }
+    if (!S.dst) {  // the side's first product
+      Rs[warp][lane] = Xa;
+      Rs[warp][lane + 32] = Xb;
+    }
+  }
+  __syncthreads();
+  if (k != 0 && warp < 6 && S.dst) {  // steps 1, 2, 4, 5: (negx ? -X : X) + sp * P
+    const int ps = warp >= 3 ? 3 : 0;
+    const uint32_t mx = S.negx ? ~0u : 0u, mp = S.sp < 0 ? ~0u : 0u, keep = S.sp != 0 ? ~0u : 0u;
+    const uint32_t c = (S.negx ? 1u : 0u) + (S.sp < 0 ? 1u : 0u);
+    Xa ^= mx;
+    Xb ^= mx;
+    lanes_add<kTwo>(Xa, Xb, (Rs[ps][lane] & keep) ^ mp, (Rs[ps][lane + 32] & keep) ^ mp, c > 0 ? 1u : 0u);
+    if (c > 1) lanes_add<kTwo>(Xa, Xb, 0u, 0u, 1u);
+    Rs[warp][lane] = Xa;
+    Rs[warp][lane + 32] = Xb;
+  }
+  __syncthreads();
+  if (k != 0) {  // m.r / m.i of each side: steps 1 / 2 (general) or 2 / 1 (k = q/2)
+    const int rstep = special ? 2 : 1, istep = special ? 1 : 2;
+    const int sa = im_in ? istep : rstep;
+    Aa = Rs[sa][lane];
+    Ab = Rs[sa][lane + 32];
+    Ba = Rs[3 + sa][lane];
+    Bb = Rs[3 + sa][lane + 32];
+  }
+  const uint32_t mi = inner_sub ? ~0u : 0u, mo = outer_sub ? ~0u : 0u;
+  lanes_add<kTwo>(Aa, Ab, Ba ^ mi, Bb ^ mi, inner_sub ? 1u : 0u);
+  lanes_add<kTwo>(Ua, Ub, Aa ^ mo, Ab ^ mo, outer_sub ? 1u : 0u);
+  lanes_st<L, kTwo>(dst, plane, Ua, Ub);
 }
 
 // ---------------------------------------------------------------------------
@@ -354,6 +493,44 @@ __global__ void __launch_bounds__(8 * kSmallBflies) mp_level_small_kernel(uint32
 // per launch) the one-thread-per-butterfly kernel is 1.5x faster.
 constexpr long long kSmallLevelButterflies = 148LL * 128;
 
+// Below this many butterflies a level runs as mp_level_warp_kernel, from 9
+// limbs up.  Whole transforms at N=1024, graph-replayed, with programmatic
+// dependent launch (us, warp kernel for every level / small kernel):
+//   one signal   4 limbs 22.6 / 20.5   9 limbs 22.6 / 26.6   17 limbs 26.7 / 35.0
+//                33 limbs 36.6 / 60.0
+//   two signals  9 limbs 25.9 / 26.7   33 limbs 45.1 / 61.5
+//   four signals 9 limbs 33.7 / 26.7   33 limbs 68.9 / 63.5  (1024 butterflies
+//                per level; 25 limbs 49.2 / 51.3 is the one case that still gains)
+// A CTA of eight warps per butterfly keeps one butterfly's latency short but
+// issues ~4x the instructions of the per-thread products, so it pays only
+// while the launch leaves most of the GPU idle.
+template <int L>
+constexpr long long warp_level_butterflies() {
+  return L >= 9 ? 640 : 0;
+}
+
+// Launches below this many butterflies (or leaves) use programmatic dependent
+// launch (pdl_wait).  Above it the early-scheduled CTAs of the next level cost
+// more than the launch latency they hide (small kernel, N=1024, 8 signals,
+// 2048 butterflies per level: 33 limbs 71.8 -> 81.7 us, 25 limbs 59.5 -> 68.7).
+constexpr long long kPdlMaxButterflies = 2048;
+
+// a launch with (pdl) or without programmatic stream serialization (pdl_wait)
+template <typename... P, typename... A>
+static cudaError_t launch_pdl(bool pdl, void (*kern)(P...), unsigned grid, unsigned block, cudaStream_t s,
+                              A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <int L>
 static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, uint32_t *out, int B,
                                  cudaStream_t s, float *launch_ms) {
@@ -362,9 +539,12 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
   {
     const long long total = (long long)T.nleaves * B;
     timer.begin();
-    if (total < kSmallLevelButterflies)
-      mp_leaf_small_kernel<L><<<(unsigned)((total + 15) / 16), 128, 0, s>>>(in, out, T.N, B, T.leaves, T.nleaves);
-    else
+    if (total < kSmallLevelButterflies) {
+      const cudaError_t e = launch_pdl(total < kPdlMaxButterflies, mp_leaf_small_kernel<L>,
+                                       (unsigned)((total + 15) / 16), 128u, s, in, out, (int)T.N, B,
+                                       (const MpLeaf *)T.leaves, (int)T.nleaves);
+      if (e != cudaSuccess) return e;
+    } else
       mp_leaf_kernel<L><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(in, out, T.N, B, T.leaves,
                                                                                     T.nleaves);
     timer.end();
@@ -375,15 +555,23 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
     const int lthreads = 128;
     const int blocks = (int)((total + lthreads - 1) / lthreads);
     timer.begin();
-    if (total < kSmallLevelButterflies)
-      mp_level_small_kernel<L><<<(unsigned)((total + kSmallBflies - 1) / kSmallBflies), 8 * kSmallBflies, 0, s>>>(
-          out, T.N, B, n, T.node_off + T.level_start[lv], T.level_count[lv], T.tw, T.dneg, T.tws);
+    const int *nodes = T.node_off + T.level_start[lv];
+    cudaError_t e = cudaSuccess;
+    const bool pdl = total < kPdlMaxButterflies;
+    if (total < warp_level_butterflies<L>())
+      e = launch_pdl(pdl, mp_level_warp_kernel<L>, (unsigned)total, (unsigned)kWarpBflyThreads, s, out, (int)T.N,
+                     B, n, nodes, (const uint32_t *)T.tw, (const uint8_t *)T.dneg, (int)T.tws);
+    else if (total < kSmallLevelButterflies)
+      e = launch_pdl(pdl, mp_level_small_kernel<L>, (unsigned)((total + kSmallBflies - 1) / kSmallBflies),
+                     (unsigned)(8 * kSmallBflies), s, out, (int)T.N, B, n, nodes, (int)T.level_count[lv],
+                     (const uint32_t *)T.tw, (const uint8_t *)T.dneg, (int)T.tws);
     else if (L <= kPackedTwiddleMaxLimbs && B % lthreads == 0)
       mp_level_kernel<L, (L <= kPackedTwiddleMaxLimbs)><<<blocks, lthreads, 0, s>>>(
           out, T.N, B, n, T.node_off + T.level_start[lv], T.level_count[lv], T.tw, T.dneg, T.tws);
     else
       mp_level_kernel<L, false><<<blocks, lthreads, 0, s>>>(out, T.N, B, n, T.node_off + T.level_start[lv],
                                                             T.level_count[lv], T.tw, T.dneg, T.tws);
+    if (e != cudaSuccess) return e;
     timer.end();
   }
   return cudaGetLastError();

@@ -115,13 +115,18 @@ def test_mp_batch_equals_single_calls(M, orc, n, p, batch):
         assert L.orc_mp_count_diff(si.ptr, yi.ptr + b * n * 32, n) == 0
 
 
-@pytest.mark.parametrize("p", [1024, 512, 100])
+# 34, 33, 32, 31, 30, 17, 4 and 2 limbs at N=1024: both sides of the
+# two-registers-per-lane boundary of the warp kernel's columns (L+2 > 32) and
+# of its limbs (L > 32)
+@pytest.mark.parametrize("p", [1060, 1024, 980, 950, 920, 512, 100, 24])
 def test_mp_small_batch_level_kernel_bit_identical(M, p):
-    """Level launches with fewer butterflies than one wave of the main level
-    kernel run one thread per product (mp_level_small_kernel).  On the same
-    limb planes, a batch of 2048 signals at N=1024 (every level on the main
-    kernel) and single signals cut from it (every level on the small kernel)
-    give bit-identical outputs."""
+    """Level launches with few butterflies run each product across a warp
+    (mp_level_warp_kernel, single signals at N=1024: at most 256 butterflies
+    per level); launches below one wave of the main level kernel run one
+    thread per product (mp_level_small_kernel).  On the same limb planes, a
+    batch of 2048 signals at N=1024 (every level on the main kernel) and
+    single signals cut from it give bit-identical outputs, and so do batches
+    of 16 (levels of up to 4096 butterflies)."""
     import torch
 
     from mpfft_b200.mparray import synthetic_planes
@@ -144,6 +149,12 @@ def test_mp_small_batch_level_kernel_bit_identical(M, p):
         plan.execute_device(1, d1.data_ptr(), o1.data_ptr(), s)
         torch.cuda.synchronize()
         assert np.array_equal(o1.cpu().numpy().view(np.uint32).reshape(2, Lm, n), big[:, :, :, b]), b
+    sub = np.ascontiguousarray(planes[:, :, :, 100:116]).reshape(-1)
+    d16 = torch.from_numpy(sub.view(np.int32)).cuda()
+    o16 = torch.empty_like(d16)
+    plan.execute_device(16, d16.data_ptr(), o16.data_ptr(), s)
+    torch.cuda.synchronize()
+    assert np.array_equal(o16.cpu().numpy().view(np.uint32).reshape(2, Lm, n, 16), big[:, :, :, 100:116])
 
 
 def test_mp_device_api_matches_host_api(M, orc):
