@@ -305,8 +305,10 @@ int mpfft_d_execute_device(mpfft_d_plan *plan, unsigned long batch, const double
  * floating tier mpfft_mp_plan_form names for that precision.  Signals are grouped into
  * one queue per form (per limb count for limbs); each queue is a persistent
  * kernel whose CTAs take whole signals, largest first, from a device counter
- * and transform them end to end, and the whole batch is captured as one CUDA
- * graph (created here, replayed by every execute).  Every output is
+ * and transform them end to end.  Limb signals of 4096 points and more form
+ * groups of equal length and limb count instead, each group one launch per
+ * stage of the transform over all its signals.  The whole batch is captured
+ * as one CUDA graph (created here, replayed by every execute).  Every output is
  * bit-identical to a single call of the same signal through
  * mpfft_mp_plan_create_flags with the same flags.  The plan owns an input and
  * an output arena in device memory holding every signal in its form's layout
@@ -344,7 +346,9 @@ int mpfft_batch_execute(mpfft_batch_plan *plan, mpfr_t *const *inr, mpfr_t *cons
 int mpfft_batch_autotune(mpfft_batch_plan *plan, int save);
 /* Queue q of the plan: family (0 limbs, 1 FP64, 2 double-double,
  * 3 quad-double, 4 float-float), limb count, CTA size, largest sub-transform,
- * signal count.  q < 0: returns the number of queues. */
+ * signal count.  The groups of long limb signals follow the queues: family 0,
+ * their limb count, CTA size 0, sub = their length.  q < 0: returns the
+ * number of queues and groups. */
 int mpfft_batch_queue_info(const mpfft_batch_plan *plan, int q, int *family, int *limbs, int *threads, int *sub,
                            int *signals);
 

@@ -2535,6 +2535,13 @@ static int family_tier(int fam) {
 }
 static int family_default_sub(int fam) { return fam == kQueueDouble ? kDSubMax : tier_sub_max(family_tier(fam)); }
 
+// Limb signals of at least this length run as groups (per-level launches over
+// every signal of one (n, L)) instead of in their queue: one CTA per signal
+// would make the longest signals the end of the launch (a 2^16-point signal
+// at 34 limbs is ~10^9 limb products on one SM) and leave the products at
+// one CTA's occupancy.
+constexpr unsigned long kGroupMinN = 4096;
+
 }  // namespace mpfft
 
 struct mpfft_batch_plan {
@@ -2552,8 +2559,17 @@ struct mpfft_batch_plan {
     std::vector<unsigned long> sigs;  // largest first
     QueueItem *d_items = nullptr;
   };
+  // long limb signals (n >= kGroupMinN): every signal of one (n, L) runs the
+  // per-level launches at once instead of one CTA per signal
+  struct Group {
+    int L = 0, tab = 0;
+    unsigned long n = 0;
+    std::vector<unsigned long> sigs;
+    QueueItem *d_items = nullptr;
+  };
   std::vector<Sig> sig;
   std::vector<Queue> queues;
+  std::vector<Group> groups;
   std::vector<QueueTables> tabs;
   QueueTables *d_tabs = nullptr;
   int *d_heads = nullptr;
@@ -2561,7 +2577,7 @@ struct mpfft_batch_plan {
   size_t arena = 0;
   std::vector<long> exps;  // limb signals: block exponents of the last host-array call
   cudaStream_t stream = nullptr;
-  std::vector<cudaStream_t> qstreams;
+  std::vector<cudaStream_t> qstreams;  // one per queue, then one per group
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> joins;
   cudaGraphExec_t graph = nullptr;
@@ -2575,6 +2591,8 @@ struct mpfft_batch_plan {
     free_graph();
     for (auto &q : queues)
       if (q.d_items) cudaFree(q.d_items);
+    for (auto &g : groups)
+      if (g.d_items) cudaFree(g.d_items);
     for (void *p : {(void *)d_tabs, (void *)d_heads, (void *)d_in, (void *)d_out})
       if (p) cudaFree(p);
     for (void *p : {(void *)h_in, (void *)h_out})
@@ -2617,7 +2635,7 @@ static int batch_capture(mpfft_batch_plan *bp) {
   CUDA_TRY(cudaMemcpy(bp->d_tabs, bp->tabs.data(), bp->tabs.size() * sizeof(QueueTables), cudaMemcpyHostToDevice));
   cudaGraph_t g = nullptr;
   CUDA_TRY(cudaStreamBeginCapture(bp->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e = cudaMemsetAsync(bp->d_heads, 0, bp->queues.size() * sizeof(int), bp->stream);
+  cudaError_t e = cudaMemsetAsync(bp->d_heads, 0, std::max<size_t>(1, bp->queues.size()) * sizeof(int), bp->stream);
   if (e == cudaSuccess) e = cudaEventRecord(bp->fork, bp->stream);
   for (size_t q = 0; q < bp->queues.size() && e == cudaSuccess; ++q) {
     const auto &Q = bp->queues[q];
@@ -2627,6 +2645,14 @@ static int batch_capture(mpfft_batch_plan *bp) {
                        bp->qstreams[q]);
     if (e == cudaSuccess) e = cudaEventRecord(bp->joins[q], bp->qstreams[q]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(bp->stream, bp->joins[q], 0);
+  }
+  for (size_t k = 0; k < bp->groups.size() && e == cudaSuccess; ++k) {
+    const auto &G = bp->groups[k];
+    const size_t b = bp->queues.size() + k;  // the group's branch
+    e = cudaStreamWaitEvent(bp->qstreams[b], bp->fork, 0);
+    if (e == cudaSuccess) e = group_launch(G.L, G.d_items, (int)G.sigs.size(), bp->tabs[G.tab], bp->qstreams[b]);
+    if (e == cudaSuccess) e = cudaEventRecord(bp->joins[b], bp->qstreams[b]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(bp->stream, bp->joins[b], 0);
   }
   const cudaError_t ce = cudaStreamEndCapture(bp->stream, &g);
   if (e == cudaSuccess) e = ce;
@@ -2728,6 +2754,7 @@ MPFFT_API int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long cou
   CUDA_TRY(cudaGetDevice(&bp->device));
   bp->sig.resize(count);
   std::map<std::pair<int, int>, int> qindex;              // (family, L) -> queue
+  std::map<std::pair<int, unsigned long>, int> gindex;    // (L, n) -> group
   std::map<std::tuple<int, int, unsigned long>, int> tindex;  // (family, L, n) -> tables
   for (unsigned long i = 0; i < count; ++i) {
     auto &s = bp->sig[i];
@@ -2757,17 +2784,6 @@ MPFFT_API int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long cou
       if (!s.mp) return g_err;
       s.bytes = (size_t)2 * s.L * s.n * 4;
     }
-    const auto qk = std::make_pair(fam, s.L);
-    if (!qindex.count(qk)) {
-      qindex[qk] = (int)bp->queues.size();
-      mpfft_batch_plan::Queue Q;
-      Q.family = fam;
-      Q.L = s.L;
-      Q.threads = fam == kQueueLimbs ? 128 : 256;
-      Q.sub = fam == kQueueLimbs ? 0 : family_default_sub(fam);
-      bp->queues.push_back(Q);
-    }
-    s.queue = qindex[qk];
     const auto tk = std::make_tuple(fam, s.L, s.n);
     if (!tindex.count(tk)) {
       tindex[tk] = (int)bp->tabs.size();
@@ -2781,6 +2797,31 @@ MPFFT_API int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long cou
       bp->tabs.push_back(t);
     }
     s.tab = tindex[tk];
+    if (fam == kQueueLimbs && s.n >= kGroupMinN) {
+      const auto gk = std::make_pair(s.L, s.n);
+      if (!gindex.count(gk)) {
+        gindex[gk] = (int)bp->groups.size();
+        mpfft_batch_plan::Group G;
+        G.L = s.L;
+        G.n = s.n;
+        G.tab = s.tab;
+        bp->groups.push_back(G);
+      }
+      s.queue = -1;
+      bp->groups[gindex[gk]].sigs.push_back(i);
+      continue;
+    }
+    const auto qk = std::make_pair(fam, s.L);
+    if (!qindex.count(qk)) {
+      qindex[qk] = (int)bp->queues.size();
+      mpfft_batch_plan::Queue Q;
+      Q.family = fam;
+      Q.L = s.L;
+      Q.threads = fam == kQueueLimbs ? 128 : 256;
+      Q.sub = fam == kQueueLimbs ? 0 : family_default_sub(fam);
+      bp->queues.push_back(Q);
+    }
+    s.queue = qindex[qk];
     bp->queues[s.queue].sigs.push_back(i);
   }
   // largest first within each queue; arena offsets queue by queue (256-byte aligned)
@@ -2794,8 +2835,13 @@ MPFFT_API int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long cou
       bp->arena += (bp->sig[i].bytes + 255) & ~(size_t)255;
     }
   }
+  for (auto &G : bp->groups)
+    for (unsigned long i : G.sigs) {
+      bp->sig[i].off = bp->arena;
+      bp->arena += (bp->sig[i].bytes + 255) & ~(size_t)255;
+    }
   CUDA_TRY(cudaMalloc(&bp->d_tabs, bp->tabs.size() * sizeof(QueueTables)));
-  CUDA_TRY(cudaMalloc(&bp->d_heads, bp->queues.size() * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&bp->d_heads, std::max<size_t>(1, bp->queues.size()) * sizeof(int)));
   if (dev_alloc((void **)&bp->d_in, bp->arena) != cudaSuccess || dev_alloc((void **)&bp->d_out, bp->arena) != cudaSuccess) {
     cudaGetLastError();
     return set_err(MPFFT_ENOMEM, "cannot allocate %zu-byte signal arenas", bp->arena);
@@ -2816,6 +2862,19 @@ MPFFT_API int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long cou
       if (bp->queues[q].family != kQueueLimbs) bp->queues[q].sub = it->second.second;
     }
     if (int e2 = batch_build_queue(bp.get(), (int)q)) return e2;
+  }
+  for (auto &G : bp->groups) {
+    cudaStream_t s;
+    cudaEvent_t e;
+    CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    bp->qstreams.push_back(s);
+    CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    bp->joins.push_back(e);
+    std::vector<QueueItem> items;
+    for (unsigned long i : G.sigs)
+      items.push_back(QueueItem{bp->d_in + bp->sig[i].off, bp->d_out + bp->sig[i].off, bp->d_tabs + G.tab});
+    CUDA_TRY(cudaMalloc(&G.d_items, items.size() * sizeof(QueueItem)));
+    CUDA_TRY(cudaMemcpy(G.d_items, items.data(), items.size() * sizeof(QueueItem), cudaMemcpyHostToDevice));
   }
   if (int e = batch_capture(bp.get())) return e;
   *plan = bp.release();
@@ -3001,8 +3060,17 @@ MPFFT_API int mpfft_batch_autotune(mpfft_batch_plan *plan, int save) {
 MPFFT_API int mpfft_batch_queue_info(const mpfft_batch_plan *plan, int q, int *family, int *limbs, int *threads,
                                      int *sub, int *signals) {
   if (!plan || !family || !limbs || !threads || !sub || !signals) return set_err(MPFFT_EINVAL, "NULL argument");
-  if (q < 0) return (int)plan->queues.size();
-  if ((size_t)q >= plan->queues.size()) return set_err(MPFFT_EINVAL, "queue %d out of range", q);
+  if (q < 0) return (int)(plan->queues.size() + plan->groups.size());
+  if ((size_t)q >= plan->queues.size() + plan->groups.size()) return set_err(MPFFT_EINVAL, "queue %d out of range", q);
+  if ((size_t)q >= plan->queues.size()) {  // a group of long limb signals: threads 0, sub = its length
+    const auto &G = plan->groups[q - plan->queues.size()];
+    *family = kQueueLimbs;
+    *limbs = G.L;
+    *threads = 0;
+    *sub = (int)G.n;
+    *signals = (int)G.sigs.size();
+    return set_err(MPFFT_OK, "");
+  }
   const auto &Q = plan->queues[q];
   *family = Q.family;
   *limbs = Q.L;

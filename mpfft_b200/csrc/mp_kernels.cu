@@ -150,14 +150,6 @@ __global__ void __launch_bounds__(128) mp_leaf_small_kernel(const uint32_t *__re
 //   k = q/2  P=(Zr+-Zi)c      m.i = (Zi-Zr)c | (Zr+Zi)c    m.r = P -> im slot
 //                                   -> re slot
 // so m.r ends in the imaginary slot and m.i in the real slot ("swapped").
-// CTAs per SM the register allocation must allow: more warps hide more
-// latency while the product still fits without spills (measured at N=1024,
-// batch 2048: 13 limbs +15 % with 6 instead of 4, 17 limbs +8.5 % with 5;
-// from 20 limbs up the smaller allocation spills).
-template <int L>
-constexpr int level_min_blocks() {
-  return L <= 14 ? 6 : (L <= 19 ? 5 : 4);
-}
 
 // Batches that are a multiple of the CTA size give every CTA one (node, k):
 // up to 31 limbs the CTA then stages its three twiddles in shared memory once

@@ -238,6 +238,10 @@ struct QueueItem {
 enum { kQueueLimbs = 0, kQueueDouble = 1, kQueueTierDD = 2, kQueueTierQD = 3, kQueueTierFF = 4 };
 cudaError_t queue_launch(int family, int L, const QueueItem *items, int nitems, int *head, int ctas, int threads,
                          double scale, cudaStream_t s);
+// Long limb signals of one (N, L): the leaf and level launches of the
+// per-level schedule over all nsig signals (items[i].in -> items[i].out, limb
+// planes of one signal each; T: the (N, L) tables with host-side level info).
+cudaError_t group_launch(int L, const QueueItem *items, int nsig, const QueueTables &T, cudaStream_t s);
 // largest resident CTAs per SM of a family's kernel at `threads` threads
 int queue_ctas_per_sm(int family, int L, int threads);
 cudaError_t queue_prepare(int family, int L);  // kernel attributes, before any stream capture

@@ -136,3 +136,42 @@ def test_queue_device_arena_scaled_inverse_and_autotune(M, orc, tmp_path, monkey
     plan.execute(ins[1], ins[0], [o[1].ptr for o in outs5], [o[0].ptr for o in outs5])
     for (n, p), a, b in zip(zip(ns, ps), outs4, outs5):
         assert L.orc_mp_count_diff(a[0].ptr, b[0].ptr, n) == 0 and L.orc_mp_count_diff(a[1].ptr, b[1].ptr, n) == 0
+
+
+def test_queue_long_limb_signals_run_as_groups(M, orc):
+    """Limb signals of 4096 points and more run as groups (per-level launches
+    over every signal of one (N, L)) instead of in their queue; their outputs
+    equal the single calls bit for bit, next to short signals of the same
+    limb counts in the queues, and the plan reports each group (threads 0,
+    sub = its length)."""
+    O = orc
+    L = O.lib()
+    spec = [(4096, 1024), (8192, 1024), (4096, 1024), (16384, 512), (4096, 100), (8192, 512),
+            (256, 1024), (1024, 512), (64, 100), (4096, 53)]
+    sig = []
+    for i, (n, p) in enumerate(spec):
+        xr, xi = O.mp_pair(n, p)
+        O.fill_uniform(xr, xi, 500 + i)
+        if i == 2:
+            L.orc_mp_scale2(xr.ptr, n, 40)
+            L.orc_mp_scale2(xi.ptr, n, 40)
+        sig.append((n, p, xr, xi))
+    plan = M.BatchPlan([s[0] for s in sig], [s[1] for s in sig], float_tiers=False)
+    groups = [q for q in plan.queues() if q["threads"] == 0]
+    assert sorted((q["sub"], q["signals"]) for q in groups) == [(4096, 1), (4096, 1), (4096, 2), (8192, 1),
+                                                                 (8192, 1), (16384, 1)], plan.queues()
+    outs = [O.mp_pair(n, p) for n, p, _, _ in sig]
+    plan.execute([s[2].ptr for s in sig], [s[3].ptr for s in sig], [o[0].ptr for o in outs],
+                 [o[1].ptr for o in outs])
+    for i, (n, p, xr, xi) in enumerate(sig):
+        single = M.MpPlan(n, p, float_tiers=False)
+        zr, zi = O.mp_pair(n, p)
+        single.execute(1, xr.ptr, xi.ptr, zr.ptr, zi.ptr)
+        assert L.orc_mp_count_diff(zr.ptr, outs[i][0].ptr, n) == 0, (i, n, p)
+        assert L.orc_mp_count_diff(zi.ptr, outs[i][1].ptr, n) == 0, (i, n, p)
+    # one grouped signal against the reference's transform at 2P bits
+    n, p, xr, xi = sig[0]
+    wr, wi = O.mp_pair(n, 2 * p)
+    O.MpFFT(n, 2 * p)(xr, xi, wr, wi)
+    e = O.mp_errors(outs[0][0], outs[0][1], wr, wi)["log2_rel"]
+    assert e <= O.mp_bound_log2(n, p), (e, O.mp_bound_log2(n, p))
