@@ -2566,6 +2566,9 @@ struct mpfft_batch_plan {
     unsigned long n = 0;
     std::vector<unsigned long> sigs;
     QueueItem *d_items = nullptr;
+    uint32_t *d_tw = nullptr;  // per-level twiddle copies (GroupTw)
+    uint8_t *d_dneg = nullptr;
+    GroupTw gt;
   };
   std::vector<Sig> sig;
   std::vector<Queue> queues;
@@ -2592,7 +2595,8 @@ struct mpfft_batch_plan {
     for (auto &q : queues)
       if (q.d_items) cudaFree(q.d_items);
     for (auto &g : groups)
-      if (g.d_items) cudaFree(g.d_items);
+      for (void *p : {(void *)g.d_items, (void *)g.d_tw, (void *)g.d_dneg})
+        if (p) cudaFree(p);
     for (void *p : {(void *)d_tabs, (void *)d_heads, (void *)d_in, (void *)d_out})
       if (p) cudaFree(p);
     for (void *p : {(void *)h_in, (void *)h_out})
@@ -2650,7 +2654,8 @@ static int batch_capture(mpfft_batch_plan *bp) {
     const auto &G = bp->groups[k];
     const size_t b = bp->queues.size() + k;  // the group's branch
     e = cudaStreamWaitEvent(bp->qstreams[b], bp->fork, 0);
-    if (e == cudaSuccess) e = group_launch(G.L, G.d_items, (int)G.sigs.size(), bp->tabs[G.tab], bp->qstreams[b]);
+    if (e == cudaSuccess)
+      e = group_launch(G.L, G.d_items, (int)G.sigs.size(), bp->tabs[G.tab], G.gt, bp->qstreams[b]);
     if (e == cudaSuccess) e = cudaEventRecord(bp->joins[b], bp->qstreams[b]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(bp->stream, bp->joins[b], 0);
   }
@@ -2875,7 +2880,17 @@ MPFFT_API int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long cou
       items.push_back(QueueItem{bp->d_in + bp->sig[i].off, bp->d_out + bp->sig[i].off, bp->d_tabs + G.tab});
     CUDA_TRY(cudaMalloc(&G.d_items, items.size() * sizeof(QueueItem)));
     CUDA_TRY(cudaMemcpy(G.d_items, items.data(), items.size() * sizeof(QueueItem), cudaMemcpyHostToDevice));
+    const QueueTables &T = bp->tabs[G.tab];
+    size_t dn = 0;
+    for (int lv = 0; lv < T.tree.nlevels; ++lv) dn += T.tree.level_n[lv] / 4;
+    if (dev_alloc((void **)&G.d_tw, std::max<size_t>(1, group_twiddle_words(G.L, T.tree)) * 4) != cudaSuccess ||
+        dev_alloc((void **)&G.d_dneg, std::max<size_t>(1, dn)) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(MPFFT_ENOMEM, "cannot allocate the twiddle copies of a group");
+    }
+    CUDA_TRY(group_twiddles(G.L, T, G.d_tw, G.d_dneg, G.gt, bp->stream));
   }
+  CUDA_TRY(cudaStreamSynchronize(bp->stream));
   if (int e = batch_capture(bp.get())) return e;
   *plan = bp.release();
   return set_err(MPFFT_OK, "");
