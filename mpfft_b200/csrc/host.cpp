@@ -2116,7 +2116,14 @@ MPFFT_API int mpfft_mp_execute_device(mpfft_mp_plan *plan, unsigned long batch, 
   if (int e = mp_big_reserve(plan, batch, &big)) return e;
   if (int e = mp_tmp_reserve(plan, batch, &tmp)) return e;
   const cudaStream_t st = (cudaStream_t)stream;
-  if (!big && !tmp && plan->rank == 1 && plan->L <= kMaxLimbs && !mp_tc_used(plan->tabs, plan->L))
+  // (not while the caller's stream is being captured: its own graph takes the launches)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    cap = cudaStreamCaptureStatusActive;
+  }
+  if (cap == cudaStreamCaptureStatusNone && !big && !tmp && plan->rank == 1 && plan->L <= kMaxLimbs &&
+      !mp_tc_used(plan->tabs, plan->L))
     if (cudaGraphExec_t ge = mp_device_graph(plan, batch, d_in, d_out)) {
       CUDA_TRY(cudaGraphLaunch(ge, st));
       return set_err(MPFFT_OK, "");
@@ -2535,11 +2542,12 @@ static int family_tier(int fam) {
 }
 static int family_default_sub(int fam) { return fam == kQueueDouble ? kDSubMax : tier_sub_max(family_tier(fam)); }
 
-// Limb signals of at least this length run as groups (per-level launches over
-// every signal of one (n, L)) instead of in their queue: one CTA per signal
-// would make the longest signals the end of the launch (a 2^16-point signal
-// at 34 limbs is ~10^9 limb products on one SM) and leave the products at
-// one CTA's occupancy.
+// Limb signals of at least this length run as groups instead of in their
+// queue: the signals of one (n, L) are transposed into the batch layout, run
+// through the batched per-level kernels as one batch, and transposed back.
+// One CTA per signal would make the longest signals the end of the launch (a
+// 2^16-point signal at 34 limbs is ~10^9 limb products on one SM) and leave
+// the products at one CTA's occupancy.
 constexpr unsigned long kGroupMinN = 4096;
 
 }  // namespace mpfft
@@ -2559,16 +2567,13 @@ struct mpfft_batch_plan {
     std::vector<unsigned long> sigs;  // largest first
     QueueItem *d_items = nullptr;
   };
-  // long limb signals (n >= kGroupMinN): every signal of one (n, L) runs the
-  // per-level launches at once instead of one CTA per signal
+  // long limb signals (n >= kGroupMinN): the signals of one (n, L) run as one
+  // batch of the per-level kernels
   struct Group {
     int L = 0, tab = 0;
     unsigned long n = 0;
-    std::vector<unsigned long> sigs;
-    QueueItem *d_items = nullptr;
-    uint32_t *d_tw = nullptr;  // per-level twiddle copies (GroupTw)
-    uint8_t *d_dneg = nullptr;
-    GroupTw gt;
+    std::vector<unsigned long> sigs;  // contiguous in the arenas, in this order
+    const mpfft_mp_plan *mp = nullptr;  // tables of (n, L)
   };
   std::vector<Sig> sig;
   std::vector<Queue> queues;
@@ -2580,7 +2585,8 @@ struct mpfft_batch_plan {
   size_t arena = 0;
   std::vector<long> exps;  // limb signals: block exponents of the last host-array call
   cudaStream_t stream = nullptr;
-  std::vector<cudaStream_t> qstreams;  // one per queue, then one per group
+  uint32_t *d_gs = nullptr;  // groups: two signal-interleaved copies of the largest group
+  std::vector<cudaStream_t> qstreams;  // one per queue, then one for the groups
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> joins;
   cudaGraphExec_t graph = nullptr;
@@ -2594,9 +2600,7 @@ struct mpfft_batch_plan {
     free_graph();
     for (auto &q : queues)
       if (q.d_items) cudaFree(q.d_items);
-    for (auto &g : groups)
-      for (void *p : {(void *)g.d_items, (void *)g.d_tw, (void *)g.d_dneg})
-        if (p) cudaFree(p);
+    if (d_gs) cudaFree(d_gs);
     for (void *p : {(void *)d_tabs, (void *)d_heads, (void *)d_in, (void *)d_out})
       if (p) cudaFree(p);
     for (void *p : {(void *)h_in, (void *)h_out})
@@ -2650,13 +2654,23 @@ static int batch_capture(mpfft_batch_plan *bp) {
     if (e == cudaSuccess) e = cudaEventRecord(bp->joins[q], bp->qstreams[q]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(bp->stream, bp->joins[q], 0);
   }
-  for (size_t k = 0; k < bp->groups.size() && e == cudaSuccess; ++k) {
-    const auto &G = bp->groups[k];
-    const size_t b = bp->queues.size() + k;  // the group's branch
-    e = cudaStreamWaitEvent(bp->qstreams[b], bp->fork, 0);
-    if (e == cudaSuccess)
-      e = group_launch(G.L, G.d_items, (int)G.sigs.size(), bp->tabs[G.tab], G.gt, bp->qstreams[b]);
-    if (e == cudaSuccess) e = cudaEventRecord(bp->joins[b], bp->qstreams[b]);
+  // the groups, one after another on one branch (each fills the GPU): the
+  // group's signals (contiguous, 2 L n words each) transposed into the
+  // batch layout, the batched transform, transposed back
+  if (!bp->groups.empty() && e == cudaSuccess) {
+    const size_t b = bp->queues.size();
+    const cudaStream_t st = bp->qstreams[b];
+    e = cudaStreamWaitEvent(st, bp->fork, 0);
+    for (const auto &G : bp->groups) {
+      if (e != cudaSuccess) break;
+      const long long W = 2LL * G.L * (long long)G.n, ns = (long long)G.sigs.size();
+      const size_t off = bp->sig[G.sigs[0]].off;
+      uint32_t *a = bp->d_gs, *c = bp->d_gs + (size_t)(W * ns);
+      e = transpose_launch(reinterpret_cast<const uint32_t *>(bp->d_in + off), a, 1, ns, W, 1, st);
+      if (e == cudaSuccess) e = mp_run_transform(G.L, G.mp->tabs, a, c, (int)ns, st, nullptr, nullptr);
+      if (e == cudaSuccess) e = transpose_launch(c, reinterpret_cast<uint32_t *>(bp->d_out + off), 1, W, ns, 1, st);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(bp->joins[b], st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(bp->stream, bp->joins[b], 0);
   }
   const cudaError_t ce = cudaStreamEndCapture(bp->stream, &g);
@@ -2810,6 +2824,7 @@ MPFFT_API int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long cou
         G.L = s.L;
         G.n = s.n;
         G.tab = s.tab;
+        G.mp = s.mp;
         bp->groups.push_back(G);
       }
       s.queue = -1;
@@ -2868,29 +2883,20 @@ MPFFT_API int mpfft_batch_plan_create(mpfft_batch_plan **plan, unsigned long cou
     }
     if (int e2 = batch_build_queue(bp.get(), (int)q)) return e2;
   }
-  for (auto &G : bp->groups) {
+  if (!bp->groups.empty()) {
     cudaStream_t s;
     cudaEvent_t e;
     CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     bp->qstreams.push_back(s);
     CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     bp->joins.push_back(e);
-    std::vector<QueueItem> items;
-    for (unsigned long i : G.sigs)
-      items.push_back(QueueItem{bp->d_in + bp->sig[i].off, bp->d_out + bp->sig[i].off, bp->d_tabs + G.tab});
-    CUDA_TRY(cudaMalloc(&G.d_items, items.size() * sizeof(QueueItem)));
-    CUDA_TRY(cudaMemcpy(G.d_items, items.data(), items.size() * sizeof(QueueItem), cudaMemcpyHostToDevice));
-    const QueueTables &T = bp->tabs[G.tab];
-    size_t dn = 0;
-    for (int lv = 0; lv < T.tree.nlevels; ++lv) dn += T.tree.level_n[lv] / 4;
-    if (dev_alloc((void **)&G.d_tw, std::max<size_t>(1, group_twiddle_words(G.L, T.tree)) * 4) != cudaSuccess ||
-        dev_alloc((void **)&G.d_dneg, std::max<size_t>(1, dn)) != cudaSuccess) {
+    size_t most = 0;
+    for (const auto &G : bp->groups) most = std::max(most, (size_t)2 * G.L * G.n * G.sigs.size());
+    if (dev_alloc((void **)&bp->d_gs, 2 * most * 4) != cudaSuccess) {
       cudaGetLastError();
-      return set_err(MPFFT_ENOMEM, "cannot allocate the twiddle copies of a group");
+      return set_err(MPFFT_ENOMEM, "cannot allocate %zu bytes of group scratch", 2 * most * 4);
     }
-    CUDA_TRY(group_twiddles(G.L, T, G.d_tw, G.d_dneg, G.gt, bp->stream));
   }
-  CUDA_TRY(cudaStreamSynchronize(bp->stream));
   if (int e = batch_capture(bp.get())) return e;
   *plan = bp.release();
   return set_err(MPFFT_OK, "");

@@ -150,9 +150,7 @@ __device__ __forceinline__ void combine(uint32_t *u0, uint32_t *u1, uint32_t *zp
 // One butterfly k of one signal b (the body of mp_level_kernel): the node of
 // size n at output offset off.  P: this thread's slot for the side's first
 // product (words ps apart); Twp: the CTA's packed twiddles (kPackedTw only).
-// kLevelTw: tw and dneg are this level's own copies, indexed by k directly
-// ([3][L][n/4] and [n/4]) instead of by k*(N/n) into the N/4-entry tables.
-template <int L, bool kPackedTw, bool kLevelTw = false>
+template <int L, bool kPackedTw>
 __device__ __forceinline__ void mp_bfly_one(uint32_t *__restrict__ y, int N, int B, int b, int n, int off, int k,
                                             const uint32_t *__restrict__ tw, const uint8_t *__restrict__ dneg,
                                             int tws, uint32_t *P, size_t ps, const uint32_t *Twp) {
@@ -168,8 +166,8 @@ __device__ __forceinline__ void mp_bfly_one(uint32_t *__restrict__ y, int N, int
     combine<L>(u0, u1, zp, zm, plane, cim, false);
     return;
   }
-  const size_t tplane = kLevelTw ? (size_t)q : (size_t)(N >> 2) * tws;  // twiddle limb-plane stride
-  const int kn = kLevelTw ? k : k * (N / n) * tws;
+  const size_t tplane = (size_t)(N >> 2) * tws;  // twiddle limb-plane stride
+  const int kn = k * (N / n) * tws;
   const uint32_t *wr = tw + kn;                           // cos
   const uint32_t *ws = tw + (size_t)L * tplane + kn;      // cos + sin
   const uint32_t *wd = tw + (size_t)2 * L * tplane + kn;  // |cos - sin|

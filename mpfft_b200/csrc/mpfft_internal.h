@@ -238,20 +238,6 @@ struct QueueItem {
 enum { kQueueLimbs = 0, kQueueDouble = 1, kQueueTierDD = 2, kQueueTierQD = 3, kQueueTierFF = 4 };
 cudaError_t queue_launch(int family, int L, const QueueItem *items, int nitems, int *head, int ctas, int threads,
                          double scale, cudaStream_t s);
-// Long limb signals of one (N, L): the leaf and level launches of the
-// per-level schedule over all nsig signals (items[i].in -> items[i].out, limb
-// planes of one signal each; T: the (N, L) tables with host-side level info;
-// gt: per-level copies of the twiddles, built by group_twiddles into
-// group_twiddle_words words and sum(n/4) bytes).
-struct GroupTw {
-  const uint32_t *tw[kMaxLevels] = {};
-  const uint8_t *dneg[kMaxLevels] = {};
-};
-size_t group_twiddle_words(int L, const TreeTables &T);
-cudaError_t group_twiddles(int L, const QueueTables &Q, uint32_t *d_tw, uint8_t *d_dneg, GroupTw &gt,
-                           cudaStream_t s);
-cudaError_t group_launch(int L, const QueueItem *items, int nsig, const QueueTables &T, const GroupTw &gt,
-                         cudaStream_t s);
 // largest resident CTAs per SM of a family's kernel at `threads` threads
 int queue_ctas_per_sm(int family, int L, int threads);
 cudaError_t queue_prepare(int family, int L);  // kernel attributes, before any stream capture

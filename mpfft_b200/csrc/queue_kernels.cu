@@ -63,55 +63,6 @@ __global__ void __launch_bounds__(256) mp_queue_kernel(const QueueItem *__restri
 }
 
 // ---------------------------------------------------------------------------
-// limb forms, long signals: a group of signals of one (N, L) runs the
-// per-level schedule over all its signals at once -- one launch for the
-// leaves, one per node size, a thread per leaf or butterfly (consecutive
-// threads consecutive k of one signal) -- instead of one CTA per signal.
-// The same device functions: bit-identical to the queue and to single calls.
-// The level launches read per-level copies of the twiddles (GroupTw), indexed
-// by k: in the N/4-entry tables consecutive k of a level of size n are N/n
-// entries apart, so a warp's twiddle loads would touch 32 sectors instead of
-// four.
-// ---------------------------------------------------------------------------
-template <int L>
-__global__ void __launch_bounds__(256) mp_group_leaf_kernel(const QueueItem *__restrict__ items, int nsig, int N,
-                                                            const MpLeaf *__restrict__ leaves, int nleaves) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)nsig * nleaves) return;
-  const QueueItem it = items[t / nleaves];
-  mp_leaf_one<L>(static_cast<const uint32_t *>(it.in), static_cast<uint32_t *>(it.out), N, 1, 0,
-                 leaves[t % nleaves]);
-}
-
-template <int L>
-__global__ void __launch_bounds__(128, level_min_blocks<L>())
-    mp_group_level_kernel(const QueueItem *__restrict__ items, int nsig, int N, int n,
-                          const int *__restrict__ node_off, int nnodes, const uint32_t *__restrict__ tw_level,
-                          const uint8_t *__restrict__ dneg_level) {
-  __shared__ uint32_t Ps[L * 128];  // each thread's first product of a side
-  const int q = n >> 2;
-  const long long per = (long long)nnodes * q;  // butterflies per signal
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)nsig * per) return;
-  const long long r = t % per;
-  uint32_t *y = static_cast<uint32_t *>(items[t / per].out);
-  mp_bfly_one<L, false, true>(y, N, 1, 0, n, node_off[r / q], (int)(r % q), tw_level, dneg_level, 1,
-                              Ps + threadIdx.x, blockDim.x, nullptr);
-}
-
-// the level copy of the twiddles: out[(r*L + i)*q + k] = tw[(r*L + i)*N/4 + k*N/n]
-__global__ void __launch_bounds__(256) mp_level_twiddle_kernel(const uint32_t *__restrict__ tw,
-                                                               const uint8_t *__restrict__ dneg, int N, int n, int L,
-                                                               uint32_t *__restrict__ out,
-                                                               uint8_t *__restrict__ dout) {
-  const int q = n >> 2;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long stride = N / n;
-  if (t < 3LL * L * q) out[t] = tw[(t / q) * (N / 4) + (t % q) * stride];
-  if (t < q) dout[t] = dneg[t * stride];
-}
-
-// ---------------------------------------------------------------------------
 // FP64: the sub-transform roots one after another in shared memory, then the
 // levels above them in global memory
 // ---------------------------------------------------------------------------
@@ -239,64 +190,6 @@ int queue_ctas_per_sm(int family, int L, int threads) {
                  cudaSuccess)
     return 1;
   return std::max(1, n);
-}
-
-size_t group_twiddle_words(int L, const TreeTables &T) {
-  size_t w = 0;
-  for (int lv = 0; lv < T.nlevels; ++lv) w += (size_t)3 * L * (T.level_n[lv] / 4);
-  return w;
-}
-
-cudaError_t group_twiddles(int L, const QueueTables &Q, uint32_t *d_tw, uint8_t *d_dneg, GroupTw &gt,
-                           cudaStream_t s) {
-  const TreeTables &T = Q.tree;
-  size_t w = 0, d = 0;
-  for (int lv = 0; lv < T.nlevels; ++lv) {
-    const int n = T.level_n[lv], q = n / 4;
-    gt.tw[lv] = d_tw + w;
-    gt.dneg[lv] = d_dneg + d;
-    const long long cnt = 3LL * L * q;
-    mp_level_twiddle_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(Q.tw, Q.dneg, Q.N, n, L, d_tw + w,
-                                                                          d_dneg + d);
-    w += (size_t)cnt;
-    d += (size_t)q;
-  }
-  return cudaGetLastError();
-}
-
-template <int L>
-static cudaError_t group_run(const QueueItem *items, int nsig, const QueueTables &Q, const GroupTw &gt,
-                             cudaStream_t s) {
-  const TreeTables &T = Q.tree;
-  const long long leaves = (long long)nsig * T.nleaves;
-  if (leaves > 0)
-    mp_group_leaf_kernel<L><<<(unsigned)((leaves + 255) / 256), 256, 0, s>>>(items, nsig, Q.N, T.leaves, T.nleaves);
-  for (int lv = 0; lv < T.nlevels; ++lv) {
-    const int n = T.level_n[lv];
-    const long long total = (long long)nsig * T.level_count[lv] * (n / 4);
-    mp_group_level_kernel<L><<<(unsigned)((total + 127) / 128), 128, 0, s>>>(
-        items, nsig, Q.N, n, T.node_off + T.level_start[lv], T.level_count[lv], gt.tw[lv], gt.dneg[lv]);
-  }
-  return cudaGetLastError();
-}
-
-cudaError_t group_launch(int L, const QueueItem *items, int nsig, const QueueTables &T, const GroupTw &gt,
-                         cudaStream_t s) {
-  if (nsig <= 0) return cudaSuccess;
-#define MPFFT_G_CASE(LL) \
-  case LL:               \
-    return group_run<LL>(items, nsig, T, gt, s);
-  switch (L) {
-    MPFFT_G_CASE(2) MPFFT_G_CASE(3) MPFFT_G_CASE(4) MPFFT_G_CASE(5) MPFFT_G_CASE(6) MPFFT_G_CASE(7)
-    MPFFT_G_CASE(8) MPFFT_G_CASE(9) MPFFT_G_CASE(10) MPFFT_G_CASE(11) MPFFT_G_CASE(12) MPFFT_G_CASE(13)
-    MPFFT_G_CASE(14) MPFFT_G_CASE(15) MPFFT_G_CASE(16) MPFFT_G_CASE(17) MPFFT_G_CASE(18) MPFFT_G_CASE(19)
-    MPFFT_G_CASE(20) MPFFT_G_CASE(21) MPFFT_G_CASE(22) MPFFT_G_CASE(23) MPFFT_G_CASE(24) MPFFT_G_CASE(25)
-    MPFFT_G_CASE(26) MPFFT_G_CASE(27) MPFFT_G_CASE(28) MPFFT_G_CASE(29) MPFFT_G_CASE(30) MPFFT_G_CASE(31)
-    MPFFT_G_CASE(32) MPFFT_G_CASE(33) MPFFT_G_CASE(34)
-    default:
-      return cudaErrorInvalidValue;
-  }
-#undef MPFFT_G_CASE
 }
 
 cudaError_t queue_launch(int family, int L, const QueueItem *items, int nitems, int *head, int ctas, int threads,

@@ -73,3 +73,34 @@ def test_two_streams_rank2_fp64_plan(M):
     torch.cuda.synchronize()
     for got, want in zip(outs, ref):
         assert torch.equal(got.cpu(), want)
+
+
+def test_device_calls_replayed_and_inside_a_callers_graph(M):
+    """A one-signal device-layout call replays its own CUDA graph from the
+    second call on, and inside a graph the caller is capturing it launches
+    its kernels into that capture instead: all give the first call's output
+    bit for bit."""
+    import torch
+
+    from mpfft_b200.mparray import synthetic_planes
+
+    n = 1024
+    plan = M.MpPlan(n, 1024)
+    host = synthetic_planes(n, plan.limbs, plan.frac_bits, 1, seed=9)
+    d_in = torch.from_numpy(host.view(np.int32)).cuda()
+    outs = [torch.empty_like(d_in) for _ in range(3)]
+    s = torch.cuda.current_stream().cuda_stream
+    for _ in range(3):  # direct, then captured and replayed
+        plan.execute_device(1, d_in.data_ptr(), outs[0].data_ptr(), s)
+    plan.execute_device(1, d_in.data_ptr(), outs[1].data_ptr(), s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(g, stream=side):
+            plan.execute_device(1, d_in.data_ptr(), outs[2].data_ptr(), side.cuda_stream)
+    g.replay()
+    torch.cuda.synchronize()
+    ref = outs[0].cpu().numpy()
+    assert np.array_equal(outs[1].cpu().numpy(), ref)
+    assert np.array_equal(outs[2].cpu().numpy(), ref)
