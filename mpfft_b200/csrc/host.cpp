@@ -20,6 +20,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <set>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -137,9 +138,11 @@ struct DeviceTree {
   TreeTables tabs;
   Leaf *d_leaves = nullptr;
   int *d_nodes = nullptr;
+  int *d_pair_nodes = nullptr;
   ~DeviceTree() {
     if (d_leaves) cudaFree(d_leaves);
     if (d_nodes) cudaFree(d_nodes);
+    if (d_pair_nodes) cudaFree(d_pair_nodes);
   }
 };
 
@@ -161,14 +164,33 @@ static int build_tree(DeviceTree &dt, unsigned long N, int leaf_max) {
     ++lv;
   }
   dt.tabs.nlevels = lv;
+  // per level: its nodes that are not the first child of a node of the next
+  // level (a first child starts at its parent's offset)
+  std::vector<int> pair_nodes;
+  for (int l = 0; l + 1 < lv; ++l) {
+    const int *up = nodes.data() + dt.tabs.level_start[l + 1];
+    std::set<int> parents(up, up + dt.tabs.level_count[l + 1]);
+    dt.tabs.pair_start[l] = (int)pair_nodes.size();
+    for (int j = 0; j < dt.tabs.level_count[l]; ++j) {
+      const int o = nodes[dt.tabs.level_start[l] + j];
+      if (!parents.count(o)) pair_nodes.push_back(o);
+    }
+    dt.tabs.pair_count[l] = (int)pair_nodes.size() - dt.tabs.pair_start[l];
+  }
   CUDA_TRY(cudaMalloc(&dt.d_leaves, sizeof(Leaf) * t.leaves.size()));
   CUDA_TRY(cudaMemcpy(dt.d_leaves, t.leaves.data(), sizeof(Leaf) * t.leaves.size(), cudaMemcpyHostToDevice));
   if (!nodes.empty()) {
     CUDA_TRY(cudaMalloc(&dt.d_nodes, sizeof(int) * nodes.size()));
     CUDA_TRY(cudaMemcpy(dt.d_nodes, nodes.data(), sizeof(int) * nodes.size(), cudaMemcpyHostToDevice));
   }
+  if (!pair_nodes.empty()) {
+    CUDA_TRY(cudaMalloc(&dt.d_pair_nodes, sizeof(int) * pair_nodes.size()));
+    CUDA_TRY(cudaMemcpy(dt.d_pair_nodes, pair_nodes.data(), sizeof(int) * pair_nodes.size(),
+                        cudaMemcpyHostToDevice));
+  }
   dt.tabs.leaves = dt.d_leaves;
   dt.tabs.node_off = dt.d_nodes;
+  dt.tabs.pair_nodes = dt.d_pair_nodes;
   return MPFFT_OK;
 }
 

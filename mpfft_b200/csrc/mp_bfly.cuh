@@ -147,6 +147,93 @@ __device__ __forceinline__ void combine(uint32_t *u0, uint32_t *u1, uint32_t *zp
 //   k = q/2  P=(Zr+-Zi)c      m.i = (Zi-Zr)c | (Zr+Zi)c    m.r = P -> im slot
 //                                   -> re slot
 // so m.r ends in the imaginary slot and m.i in the real slot ("swapped").
+//
+// The six twiddle steps of butterfly k != 0 of one signal, without the
+// combine: the products of the Z+ slots (zp) and Z- slots (zm) by w^k and
+// w^-k, merged and stored back into the slots swapped (m.r in the imaginary
+// slot, m.i in the real one).  n: the node size (q = n/4); P: this thread's
+// slot for the side's first product (words ps apart); Twp: the CTA's packed
+// twiddles (kPackedTw only).  The merged products are stored with L2 priority
+// evict_last (a fused thread of mp_level_pair_kernel reads them back only
+// after two more butterflies).  mp_bfly_one below spells out the same steps
+// inline (its register allocation at 33 limbs spills less that way); the
+// kernels built on each are checked to be bit-identical.
+template <int L, bool kPackedTw>
+__device__ __forceinline__ void mp_bfly_steps(uint32_t *zp, uint32_t *zm, size_t plane, size_t cim, int N, int n,
+                                              int k, const uint32_t *__restrict__ tw,
+                                              const uint8_t *__restrict__ dneg, int tws, uint32_t *P, size_t ps,
+                                              const uint32_t *Twp) {
+  const int q = n >> 2;
+  const size_t tplane = (size_t)(N >> 2) * tws;  // twiddle limb-plane stride
+  const int kn = k * (N / n) * tws;
+  const uint32_t *wr = tw + kn;                           // cos
+  const uint32_t *ws = tw + (size_t)L * tplane + kn;      // cos + sin
+  const uint32_t *wd = tw + (size_t)2 * L * tplane + kn;  // |cos - sin|
+  const bool special = (2 * k == q);
+  const bool dn = special ? false : (dneg[kn] != 0);
+  constexpr int Lp = (L + 3) & ~3;  // packed twiddle stride: 16-byte aligned rows
+  uint32_t X[L];
+#pragma unroll 1
+  for (int st_ = 0; st_ < 6; ++st_) {
+    const int side = st_ >= 3;
+    const int step = st_ - 3 * side;
+    uint32_t *zr = side ? zm : zp;
+    uint32_t *zi = zr + cim;
+    const uint32_t *pa = zr, *pb = nullptr, *w = wr;
+    int wsel = 0;  // packed twiddle row: 0 cos, 1 cos+sin, 2 |cos-sin|
+    bool sub = false, negx = false, mul = true;
+    int sp = 0;
+    uint32_t *dst = nullptr;  // null: the product becomes P
+    if (step == 0) {
+      pb = zi;
+      sub = side;
+    } else if (!special) {
+      if (step == 1) {
+        pa = zi;
+        w = wd;
+        wsel = 2;
+        negx = dn ^ (side == 0);
+        sp = 1;
+        dst = zi;
+      } else {
+        w = ws;
+        wsel = 1;
+        negx = (side == 0);
+        sp = side ? -1 : 1;
+        dst = zr;
+      }
+    } else {
+      if (step == 1) {
+        pa = side ? zr : zi;
+        pb = side ? zi : zr;
+        sub = !side;
+        dst = zr;
+      } else {
+        mul = false;
+        sp = 1;
+        dst = zi;
+      }
+    }
+    if (mul) {
+      ld_addsub<L>(X, pa, pb, plane, sub);
+      if (kPackedTw) mul_tw<L, true>(X, Twp + wsel * Lp, 0);
+      else mul_tw<L>(X, w, tplane);
+    } else {
+#pragma unroll
+      for (int i = 0; i < L; ++i) X[i] = 0;
+    }
+    if (!dst) {
+      st<L>(P, ps, X);
+    } else {
+      combine_p<L>(X, P, ps, negx, sp);
+      // the merged product is read again by the combine: keep it in L2
+      const uint64_t keep = l2_policy_evict_last();
+#pragma unroll
+      for (int i = 0; i < L; ++i) st_hint(dst + (size_t)i * plane, X[i], keep);
+    }
+  }
+}
+
 // One butterfly k of one signal b (the body of mp_level_kernel): the node of
 // size n at output offset off.  P: this thread's slot for the side's first
 // product (words ps apart); Twp: the CTA's packed twiddles (kPackedTw only).

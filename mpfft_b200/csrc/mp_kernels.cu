@@ -187,6 +187,132 @@ __global__ void __launch_bounds__(128, level_min_blocks<L>()) mp_level_kernel(ui
 }
 
 // ---------------------------------------------------------------------------
+// two levels in one launch: a node of size 2n together with its first child
+// ---------------------------------------------------------------------------
+//
+// A node Y of size 2n (quarter 2q, q = n/4) at offset off has as first child
+// the node X of size n at the same offset, so X's butterfly k writes X[k],
+// X[k+q], X[k+2q], X[k+3q] -- exactly the U inputs of Y's butterflies k
+// (U0 = Y[k], U1 = Y[k+2q]) and k+q (U0 = Y[k+q], U1 = Y[k+3q]).  One thread
+// runs all three butterflies of one signal: the twiddle steps of each (the
+// products land in their Z slots as in mp_level_kernel), then one streamed
+// pass of the three L-combines, in which X's outputs go straight into Y's
+// combines and are never stored.  Per level pair the planes cross HBM once
+// instead of twice, and a thread's loads and stores drop from 3 x 28 L to
+// 68 L words.  The same modular sums and products of the same operands as
+// two mp_level_kernel launches, so the results are bit-identical.
+//
+// Nodes of size n that are not a first child (the conjugate-pair children of
+// nodes of size 4n) run in the same launch as ordinary butterflies, after the
+// fused ones: thread t < ny*q*B is fused, the rest take unodes.
+
+// Twelve carry chains of one L-combine (the operations of combine()), one limb
+// at a time: o = u0r, zpr, u1r, zmr, u0i, zpi, u1i, zmi of that limb.
+struct CombineChains {
+  uint32_t ca1r = 0, ca1i = 0, ca2r = 1, ca2i = 1;
+  uint32_t c0r = 0, c2r = 1, c1r = 0, c3r = 1, c0i = 0, c2i = 1, c1i = 1, c3i = 0;
+  __device__ __forceinline__ void limb(uint32_t U0r, uint32_t U0i, uint32_t U1r, uint32_t U1i, uint32_t m1r,
+                                       uint32_t m1i, uint32_t m2r, uint32_t m2i, uint32_t (&o)[8]) {
+    const uint32_t a1r = addc(m1r, m2r, ca1r), a1i = addc(m1i, m2i, ca1i);
+    const uint32_t a2r = addc(m1r, ~m2r, ca2r), a2i = addc(m1i, ~m2i, ca2i);
+    o[0] = addc(U0r, a1r, c0r);
+    o[1] = addc(U0r, ~a1r, c2r);
+    o[2] = addc(U1r, a2i, c1r);
+    o[3] = addc(U1r, ~a2i, c3r);
+    o[4] = addc(U0i, a1i, c0i);
+    o[5] = addc(U0i, ~a1i, c2i);
+    o[6] = addc(U1i, ~a2r, c1i);
+    o[7] = addc(U1i, a2r, c3i);
+  }
+};
+
+// Limb counts up to which combine_pair's limb loop is unrolled; above, the
+// unrolled loop's register demand next to the 128-register product costs more
+// than it saves, and the rolled loop reads the Z slots through ld_hint (kept
+// in program order; 33 limbs 3.02 -> 2.91 ms, 9 and 17 limbs 6 % slower that
+// way).  N=1024, batch 2048, ms per transform batch, unrolled / rolled with
+// plain loads: 9 limbs 0.517 / 0.601, 17 limbs 1.091 / 1.186, 25 limbs 1.886 /
+// 1.886, 29 limbs 2.479 / 2.337, 33 limbs 3.265 / 3.010, 34 limbs 3.489 / 3.279.
+constexpr int kPairUnrollMaxLimbs = 25;
+
+// One limb of the three L-combines of a fused thread; p: limb i of position k
+// of the pair's node Y (word stride qB = q*B between the positions k + j*q).
+// X's Z slots are at 2q, 3q; Y_k's at 4q, 6q; Y_{k+q}'s at 5q, 7q (always
+// twiddled: swapped).  The outputs are stored with L2 priority evict_first:
+// the next launch reads them after the whole signal has passed through L2.
+template <bool kOrderedLoads>
+__device__ __forceinline__ void combine_pair_limb(uint32_t *p, size_t qB, size_t cim, size_t sre, size_t sim,
+                                                  CombineChains &cx, CombineChains &cy0, CombineChains &cy1,
+                                                  uint64_t ld_pol, uint64_t st_pol) {
+  auto z = [&](size_t o) { return kOrderedLoads ? ld_hint(p + o, ld_pol) : p[o]; };
+  uint32_t ox[8], o0[8], o1[8];
+  cx.limb(p[0], p[cim], p[qB], p[qB + cim], z(2 * qB + sre), z(2 * qB + sim), z(3 * qB + sre), z(3 * qB + sim), ox);
+  cy0.limb(ox[0], ox[4], ox[1], ox[5], z(4 * qB + sre), z(4 * qB + sim), z(6 * qB + sre), z(6 * qB + sim), o0);
+  cy1.limb(ox[2], ox[6], ox[3], ox[7], z(5 * qB + cim), z(5 * qB), z(7 * qB + cim), z(7 * qB), o1);
+  const uint32_t *v0 = o0, *v1 = o1;
+  // output j of Y_k / Y_{k+q} (u0, zp, u1, zm) at positions 0, 4q, 2q, 6q / q, 5q, 3q, 7q
+  const int pos0[4] = {0, 4, 2, 6}, pos1[4] = {1, 5, 3, 7};
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    st_hint(p + pos0[j] * qB, v0[j], st_pol);
+    st_hint(p + pos0[j] * qB + cim, v0[j + 4], st_pol);
+    st_hint(p + pos1[j] * qB, v1[j], st_pol);
+    st_hint(p + pos1[j] * qB + cim, v1[j + 4], st_pol);
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void combine_pair(uint32_t *p, size_t qB, size_t plane, size_t cim, bool swapped) {
+  const size_t sre = swapped ? cim : 0, sim = swapped ? 0 : cim;
+  const uint64_t st_pol = l2_policy_evict_first();
+  CombineChains cx, cy0, cy1;
+  if constexpr (L <= kPairUnrollMaxLimbs) {
+#pragma unroll
+    for (int i = 0; i < L; ++i, p += plane)
+      combine_pair_limb<false>(p, qB, cim, sre, sim, cx, cy0, cy1, 0, st_pol);
+  } else {
+    const uint64_t ld_pol = l2_policy_evict_normal();
+#pragma unroll 1
+    for (int i = 0; i < L; ++i, p += plane)
+      combine_pair_limb<true>(p, qB, cim, sre, sim, cx, cy0, cy1, ld_pol, st_pol);
+  }
+}
+
+template <int L>
+__global__ void __launch_bounds__(128, level_min_blocks<L>()) mp_level_pair_kernel(
+    uint32_t *__restrict__ y, int N, int B, int n, const int *__restrict__ ynodes, int ny,
+    const int *__restrict__ unodes, int nu, const uint32_t *__restrict__ tw, const uint8_t *__restrict__ dneg,
+    int tws) {
+  __shared__ uint32_t Ps[L * 128];
+  const int q = n >> 2;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nf = (long long)ny * q * B;
+  const bool fused = t < nf;
+  const long long u = fused ? t : t - nf;
+  if (!fused && u >= (long long)nu * q * B) return;
+  const int b = (int)(u % B);
+  const long long r = u / B;
+  const int k = (int)(r % q);
+  const int off = fused ? ynodes[r / q] : unodes[r / q];
+  const size_t plane = (size_t)N * B;
+  const size_t cim = (size_t)L * plane;
+  const size_t qB = (size_t)q * B;
+  uint32_t *p = y + (size_t)(off + k) * B + b;
+  // the twiddle steps: X's (or the unfused node's) butterfly k, then Y's
+  // butterflies k and k+q; one inlined copy of the product
+#pragma unroll 1
+  for (int j = 0; j < (fused ? 3 : 1); ++j) {
+    const int kk = j == 2 ? k + q : k;
+    if (kk == 0) continue;
+    const int zs = j == 0 ? 2 : (j == 1 ? 4 : 5);  // Z+ slot at zs*q, Z- at (zs+1)*q or (zs+2)*q
+    mp_bfly_steps<L, false>(p + (size_t)zs * qB, p + (size_t)(j == 0 ? 3 : zs + 2) * qB, plane, cim, N,
+                            j == 0 ? n : 2 * n, kk, tw, dneg, tws, Ps + threadIdx.x, blockDim.x, nullptr);
+  }
+  if (fused) combine_pair<L>(p, qB, plane, cim, k != 0);
+  else combine<L>(p, p + qB, p + 2 * qB, p + 3 * qB, plane, cim, k != 0);
+}
+
+// ---------------------------------------------------------------------------
 // the same launch for batches too small to fill the GPU
 // ---------------------------------------------------------------------------
 //
@@ -485,6 +611,16 @@ __global__ void __launch_bounds__(kWarpBflyThreads) mp_level_warp_kernel(uint32_
 // per launch) the one-thread-per-butterfly kernel is 1.5x faster.
 constexpr long long kSmallLevelButterflies = 148LL * 128;
 
+// Two levels run as one mp_level_pair_kernel launch when its fused threads
+// (three butterflies each) fill at least one wave of the GPU; with fewer the
+// single-level launches keep more butterflies in flight (N=1024, batch 256,
+// where the top pair has 32768 fused threads: 3, 5, 9 and 17 limbs 4 %, 4.6 %,
+// 5.6 % and 2.5 % slower as pairs, 33 limbs 0.6 % faster).
+template <int L>
+constexpr long long pair_min_fused_threads() {
+  return 148LL * 128 * level_min_blocks<L>();
+}
+
 // Below this many butterflies a level runs as mp_level_warp_kernel, from 9
 // limbs up.  Whole transforms at N=1024, graph-replayed, with programmatic
 // dependent launch (us, warp kernel for every level / small kernel):
@@ -546,6 +682,19 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
     const long long total = (long long)T.level_count[lv] * (n / 4) * B;
     const int lthreads = 128;
     const int blocks = (int)((total + lthreads - 1) / lthreads);
+    const long long fused = lv + 1 < T.nlevels ? (long long)T.level_count[lv + 1] * (n / 4) * B : 0;
+    if (fused >= pair_min_fused_threads<L>()) {
+      // levels lv and lv+1 in one launch; lv+1's timer entry stays 0
+      const long long threads = fused + (long long)T.pair_count[lv] * (n / 4) * B;
+      timer.begin();
+      mp_level_pair_kernel<L><<<(unsigned)((threads + lthreads - 1) / lthreads), lthreads, 0, s>>>(
+          out, T.N, B, n, T.node_off + T.level_start[lv + 1], T.level_count[lv + 1],
+          T.pair_nodes + T.pair_start[lv], T.pair_count[lv], T.tw, T.dneg, T.tws);
+      timer.end();
+      timer.none();
+      ++lv;
+      continue;
+    }
     timer.begin();
     const int *nodes = T.node_off + T.level_start[lv];
     cudaError_t e = cudaSuccess;

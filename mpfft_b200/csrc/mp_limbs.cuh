@@ -20,6 +20,35 @@
 
 namespace mpfft {
 
+// L2 eviction priorities for global accesses (cache-policy operands of
+// ld/st ... .L2::cache_hint): evict_last keeps a line that will be read again
+// soon, evict_first marks a line that will not be read before it leaves L2.
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_normal() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void st_hint(uint32_t *a, uint32_t v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(a), "r"(v), "l"(pol) : "memory");
+}
+// (asm volatile: the compiler keeps these loads in program order, which also
+// stops it from hoisting them far ahead of their use)
+__device__ __forceinline__ uint32_t ld_hint(const uint32_t *a, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol) : "memory");
+  return v;
+}
+
 // one step of a carry chain: returns a + b + c (mod 2^32), c <- carry out
 __device__ __forceinline__ uint32_t addc(uint32_t a, uint32_t b, uint32_t &c) {
   const uint64_t t = (uint64_t)a + b + c;

@@ -35,6 +35,12 @@ struct TreeTables {
   int level_start[kMaxLevels] = {};
   int level_count[kMaxLevels] = {};
   const int *node_off = nullptr;
+  // for a launch of levels lv and lv+1 together (mp_level_pair_kernel): the
+  // nodes of size level_n[lv] that are not the first child of a node of size
+  // level_n[lv+1], at pair_nodes + pair_start[lv] (pair_count[lv] of them)
+  const int *pair_nodes = nullptr;
+  int pair_start[kMaxLevels] = {};
+  int pair_count[kMaxLevels] = {};
 };
 
 struct MpDeviceTables : TreeTables {
@@ -60,6 +66,12 @@ struct SubSchedule {
   int level_start[kMaxLevels] = {};
   int level_count[kMaxLevels] = {};
   const int *node_off = nullptr;
+  // for a launch of levels lv and lv+1 together (mp_level_pair_kernel): the
+  // nodes of size level_n[lv] that are not the first child of a node of size
+  // level_n[lv+1], at pair_nodes + pair_start[lv] (pair_count[lv] of them)
+  const int *pair_nodes = nullptr;
+  int pair_start[kMaxLevels] = {};
+  int pair_count[kMaxLevels] = {};
 };
 
 // root of a shared-memory sub-transform: input elements x[(sn + j*s)] (j = 0
@@ -136,10 +148,17 @@ struct LaunchTimer {
     cudaEventRecord(ev[2 * n + 1], s);
     ++n;
   }
+  // an entry without a launch of its own (a level run together with the previous one): 0 ms
+  void none() {
+    if (!ms) return;
+    ++n;
+  }
   ~LaunchTimer() {
     if (!ms) return;
     cudaStreamSynchronize(s);
     for (int i = 0; i < n; ++i) {
+      ms[i] = 0.0f;
+      if (!ev[2 * i]) continue;
       cudaEventElapsedTime(&ms[i], ev[2 * i], ev[2 * i + 1]);
       cudaEventDestroy(ev[2 * i]);
       cudaEventDestroy(ev[2 * i + 1]);

@@ -124,7 +124,8 @@ def test_mp_small_batch_level_kernel_bit_identical(M, p):
     (mp_level_warp_kernel, single signals at N=1024: at most 256 butterflies
     per level); launches below one wave of the main level kernel run one
     thread per product (mp_level_small_kernel).  On the same limb planes, a
-    batch of 2048 signals at N=1024 (every level on the main kernel) and
+    batch of 2048 signals at N=1024 (every level pair in one launch of
+    mp_level_pair_kernel) and
     single signals cut from it give bit-identical outputs, and so do batches
     of 16 (levels of up to 4096 butterflies)."""
     import torch
@@ -155,6 +156,43 @@ def test_mp_small_batch_level_kernel_bit_identical(M, p):
     plan.execute_device(16, d16.data_ptr(), o16.data_ptr(), s)
     torch.cuda.synchronize()
     assert np.array_equal(o16.cpu().numpy().view(np.uint32).reshape(2, Lm, n, 16), big[:, :, :, 100:116])
+
+
+# (n, precision, batch): 33 limbs (rolled combine loop) and 9, 10, 17, 25
+# limbs (unrolled); batches that are not a multiple of the CTA size, so one
+# CTA holds fused and unfused butterflies; n = 2048 has an odd number of
+# levels (the top one runs alone); n = 16 is one level pair and nothing else.
+# Each batch gives every pair at least one wave of fused threads.
+@pytest.mark.parametrize("n,p,B", [(1024, 1024, 1000), (1024, 512, 1200), (1024, 760, 2000), (2048, 256, 900),
+                                   (16, 1024, 40000), (64, 300, 20000)])
+def test_mp_level_pairs_bit_identical(M, n, p, B):
+    """Batches large enough for the main level kernel run two levels per
+    launch (mp_level_pair_kernel: each node with its first child, the child's
+    outputs fed into the parent's combine without a store).  Single signals
+    cut from the batch run every level on its own (warp-parallel and
+    small-batch kernels): the outputs are bit-identical."""
+    import torch
+
+    from mpfft_b200.mparray import synthetic_planes
+
+    plan = M.MpPlan(n, p)
+    Lm = plan.limbs
+    host = synthetic_planes(n, Lm, plan.frac_bits, B, seed=11)
+    s = torch.cuda.current_stream().cuda_stream
+    d_in = torch.from_numpy(host.view(np.int32)).cuda()
+    d_out = torch.empty_like(d_in)
+    ms = plan.execute_device_timed(B, d_in.data_ptr(), d_out.data_ptr(), s)
+    torch.cuda.synchronize()
+    assert ms[1:].count(0.0) == len(ms[1:]) // 2, "not every level pair ran as one launch"
+    big = d_out.cpu().numpy().view(np.uint32).reshape(2, Lm, n, B)
+    planes = host.reshape(2, Lm, n, B)
+    for b in (0, 127, 128, B // 2, B - 1):
+        one = np.ascontiguousarray(planes[:, :, :, b]).reshape(-1)
+        d1 = torch.from_numpy(one.view(np.int32)).cuda()
+        o1 = torch.empty_like(d1)
+        plan.execute_device(1, d1.data_ptr(), o1.data_ptr(), s)
+        torch.cuda.synchronize()
+        assert np.array_equal(o1.cpu().numpy().view(np.uint32).reshape(2, Lm, n), big[:, :, :, b]), b
 
 
 def test_mp_device_api_matches_host_api(M, orc):
