@@ -197,23 +197,55 @@ __device__ __forceinline__ void d_butterfly(double *yr, double *yi, size_t strid
   i0[3 * qs] = (u1i + dr) * scale;
 }
 
+// 4m2a butterfly on values in registers: (U0, U1, Z+, Z-) -> the outputs that
+// go to the same four positions (the operations of d_butterfly)
+struct DCplx {
+  double r, i;
+};
+__device__ __forceinline__ void d_bfly_vals(DCplx &u0, DCplx &u1, DCplx &zp, DCplx &zm, double w_r, double w_i,
+                                            double scale) {
+  const double pr = w_r * zp.r + w_i * zp.i, pi = w_r * zp.i - w_i * zp.r;
+  const double mr = w_r * zm.r - w_i * zm.i, mi = w_r * zm.i + w_i * zm.r;
+  const double sr = pr + mr, si = pi + mi, dr = pr - mr, di = pi - mi;
+  const DCplx a = u0, b = u1;
+  u0 = DCplx{(a.r + sr) * scale, (a.i + si) * scale};
+  zp = DCplx{(a.r - sr) * scale, (a.i - si) * scale};
+  u1 = DCplx{(b.r + di) * scale, (b.i - dr) * scale};
+  zm = DCplx{(b.r - di) * scale, (b.i + dr) * scale};
+}
+
 // 4m2a butterfly in shared memory (padded indices)
 __device__ __forceinline__ void d_butterfly_smem(double *yr, double *yi, int off, int k, int q, double w_r,
                                                  double w_i, double scale) {
-  const int a0 = pidx(off + k), a1 = pidx(off + k + q), a2 = pidx(off + k + 2 * q), a3 = pidx(off + k + 3 * q);
-  const double u0r = yr[a0], u1r = yr[a1], zpr = yr[a2], zmr = yr[a3];
-  const double u0i = yi[a0], u1i = yi[a1], zpi = yi[a2], zmi = yi[a3];
-  const double pr = w_r * zpr + w_i * zpi, pi = w_r * zpi - w_i * zpr;
-  const double mr = w_r * zmr - w_i * zmi, mi = w_r * zmi + w_i * zmr;
-  const double sr = pr + mr, si = pi + mi, dr = pr - mr, di = pi - mi;
-  yr[a0] = (u0r + sr) * scale;
-  yr[a2] = (u0r - sr) * scale;
-  yr[a1] = (u1r + di) * scale;
-  yr[a3] = (u1r - di) * scale;
-  yi[a0] = (u0i + si) * scale;
-  yi[a2] = (u0i - si) * scale;
-  yi[a1] = (u1i - dr) * scale;
-  yi[a3] = (u1i + dr) * scale;
+  const int a[4] = {pidx(off + k), pidx(off + k + q), pidx(off + k + 2 * q), pidx(off + k + 3 * q)};
+  DCplx v[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) v[j] = DCplx{yr[a[j]], yi[a[j]]};
+  d_bfly_vals(v[0], v[1], v[2], v[3], w_r, w_i, scale);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) yr[a[j]] = v[j].r, yi[a[j]] = v[j].i;
+}
+
+// Two levels of one node in shared memory: butterfly k of the first child X
+// (size n, q = n/4, at the node's offset) and butterflies k and k+q of the node
+// Y (size 2n), whose U inputs are exactly X's four outputs -- they stay in
+// registers between the two levels.  wx: X's twiddle; wy0, wy1: Y's for k and
+// k+q; scale applies to Y's outputs.
+__device__ __forceinline__ void d_bfly_pair_smem(double *yr, double *yi, int off, int k, int q, double wx_r,
+                                                 double wx_i, double wy0_r, double wy0_i, double wy1_r,
+                                                 double wy1_i, double scale) {
+  int a[8];
+  DCplx v[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    a[j] = pidx(off + k + j * q);
+    v[j] = DCplx{yr[a[j]], yi[a[j]]};
+  }
+  d_bfly_vals(v[0], v[1], v[2], v[3], wx_r, wx_i, 1.0);
+  d_bfly_vals(v[0], v[2], v[4], v[6], wy0_r, wy0_i, scale);
+  d_bfly_vals(v[1], v[3], v[5], v[7], wy1_r, wy1_i, scale);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) yr[a[j]] = v[j].r, yi[a[j]] = v[j].i;
 }
 
 // One CTA = G instances (sub-transform root x signal) entirely in shared
@@ -289,10 +321,36 @@ __device__ __forceinline__ void d_sub_instances(const double *__restrict__ in, d
       yi[pidx(m)] *= scale;
     }
   }
-  // levels (the small schedule's levels are the big one's minus the last)
+  // levels (the small schedule's levels are the big one's minus the last),
+  // two per pass: each node of the upper level with its first child, then the
+  // lower level's other nodes; an odd top level runs alone
+  const SubSchedule &S = is_big ? big : small;
   for (int lv = 0; lv < nlevels; ++lv) {
     __syncthreads();
     const int n = big.level_n[lv], q = n >> 2, lgq = 29 - __clz(n);
+    if (lv + 1 < nlevels) {
+      const int cy = S.level_count[lv + 1], cu = S.pair_count[lv];
+      const int *ynodes = S.node_off + S.level_start[lv + 1], *unodes = S.pair_nodes + S.pair_start[lv];
+      const int per = (cy + cu) * q;
+      const double sc = lv + 1 == nlevels - 1 ? scale : 1.0;
+      for (int e = threadIdx.x; e < G_here * per; e += blockDim.x) {
+        const int g = SINGLE ? e / per : 0, t = SINGLE ? e - g * per : e;
+        const int node = t >> lgq, k = t & (q - 1);
+        const int km = k << (lgT - (lgq + 2));  // k * (T/n)
+        double *yr = sm + (size_t)g * istride, *yi = yr + Tmax;
+        if (node < cy) {
+          const int ky0 = k << (lgT - (lgq + 3)), ky1 = (k + q) << (lgT - (lgq + 3));  // k * (T/2n), (k+q) * (T/2n)
+          d_bfly_pair_smem(yr, yi, ynodes[node], k, q, __ldg(wr + (size_t)km * tws), __ldg(wi + (size_t)km * tws),
+                           __ldg(wr + (size_t)ky0 * tws), __ldg(wi + (size_t)ky0 * tws),
+                           __ldg(wr + (size_t)ky1 * tws), __ldg(wi + (size_t)ky1 * tws), sc);
+        } else {
+          d_butterfly_smem(yr, yi, unodes[node - cy], k, q, __ldg(wr + (size_t)km * tws),
+                           __ldg(wi + (size_t)km * tws), 1.0);
+        }
+      }
+      ++lv;
+      continue;
+    }
     const int cnt = is_big ? big.level_count[lv] : small.level_count[lv];
     const int *nodes = (is_big ? big.node_off : small.node_off) + (is_big ? big.level_start[lv] : small.level_start[lv]);
     const int per = cnt * q;

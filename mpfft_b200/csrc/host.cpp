@@ -1371,9 +1371,23 @@ static int build_sub(mpfft_d_plan *p, int size, SubSchedule &S, int leaf_max = 1
     nodes.insert(nodes.end(), kv.second.begin(), kv.second.end());
     ++S.nlevels;
   }
+  // per level: its nodes that are not the first child of a node of the next
+  // level (a first child starts at its parent's offset)
+  std::vector<int> pair_nodes;
+  for (int l = 0; l + 1 < S.nlevels; ++l) {
+    const int *up = nodes.data() + S.level_start[l + 1];
+    std::set<int> parents(up, up + S.level_count[l + 1]);
+    S.pair_start[l] = (int)pair_nodes.size();
+    for (int j = 0; j < S.level_count[l]; ++j) {
+      const int o = nodes[S.level_start[l] + j];
+      if (!parents.count(o)) pair_nodes.push_back(o);
+    }
+    S.pair_count[l] = (int)pair_nodes.size() - S.pair_start[l];
+  }
   if (int e = upload(p, perm, &S.perm)) return e;
   if (int e = upload(p, t.leaves, &S.leaves)) return e;
   if (int e = upload(p, nodes, &S.node_off)) return e;
+  if (int e = upload(p, pair_nodes, &S.pair_nodes)) return e;
   return MPFFT_OK;
 }
 

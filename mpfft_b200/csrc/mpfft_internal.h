@@ -66,9 +66,9 @@ struct SubSchedule {
   int level_start[kMaxLevels] = {};
   int level_count[kMaxLevels] = {};
   const int *node_off = nullptr;
-  // for a launch of levels lv and lv+1 together (mp_level_pair_kernel): the
-  // nodes of size level_n[lv] that are not the first child of a node of size
-  // level_n[lv+1], at pair_nodes + pair_start[lv] (pair_count[lv] of them)
+  // for levels lv and lv+1 run in one pass (each node of size level_n[lv+1]
+  // with its first child): the nodes of size level_n[lv] that are not a first
+  // child, at pair_nodes + pair_start[lv] (pair_count[lv] of them)
   const int *pair_nodes = nullptr;
   int pair_start[kMaxLevels] = {};
   int pair_count[kMaxLevels] = {};
