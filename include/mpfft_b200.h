@@ -393,7 +393,9 @@ size_t mpfft_static_scratch_bytes(void);
  * butterfly launch (after the one leaf launch).  Returns the level count. */
 int mpfft_mp_plan_schedule(const mpfft_mp_plan *plan, int *level_n, int *level_nodes, int max_levels);
 /* mpfft_mp_execute_device with every launch bracketed by CUDA events on
- * `stream`; launch_ms[0] = leaf launch, launch_ms[1+i] = level i.  Synchronous. */
+ * `stream`; launch_ms[0] = leaf launch, launch_ms[1+i] = level i.  A level
+ * that ran in one launch with level i-1 (large batches: two levels per
+ * launch) reads 0 and the launch's time is in level i-1's entry.  Synchronous. */
 int mpfft_mp_execute_device_timed(mpfft_mp_plan *plan, unsigned long batch, const uint32_t *d_in,
                                   uint32_t *d_out, void *stream, float *launch_ms);
 /* Measured integer multiply-add rate of the current GPU (ops/s): wide = 0 for

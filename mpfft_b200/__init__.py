@@ -254,7 +254,8 @@ class MpPlan:
         return [(a[i], b[i]) for i in range(max(k, 0))]
 
     def execute_device_timed(self, batch, d_in: int, d_out: int, stream: int = 0) -> list[float]:
-        """Per-launch durations (ms): [leaf, level 0, level 1, ...]."""
+        """Per-launch durations (ms): [leaf, level 0, level 1, ...]; a level
+        that ran in one launch with the level before it reads 0.0."""
         nl = len(self.schedule())
         ms = (C.c_float * (nl + 1))()
         _check(lib.mpfft_mp_execute_device_timed(self.h, batch, d_in, d_out, stream or None, ms))
