@@ -278,8 +278,18 @@ __device__ __forceinline__ void combine_pair(uint32_t *p, size_t qB, size_t plan
   }
 }
 
+// CTAs per SM of mp_level_pair_kernel: from 31 limbs three (up to 170
+// registers, no spills) instead of the one-level kernel's four, whose
+// 128-register product spills (N=1024, batch 2048, ms per batch, four / three
+// CTAs: 21 limbs 1.435 / 1.519, 25 1.837 / 1.929, 29 2.299 / 2.319, 31 2.706 /
+// 2.638, 33 2.913 / 2.833, 34 3.257 / 3.005).
 template <int L>
-__global__ void __launch_bounds__(128, level_min_blocks<L>()) mp_level_pair_kernel(
+constexpr int pair_min_blocks() {
+  return L >= 31 ? 3 : level_min_blocks<L>();
+}
+
+template <int L>
+__global__ void __launch_bounds__(128, pair_min_blocks<L>()) mp_level_pair_kernel(
     uint32_t *__restrict__ y, int N, int B, int n, const int *__restrict__ ynodes, int ny,
     const int *__restrict__ unodes, int nu, const uint32_t *__restrict__ tw, const uint8_t *__restrict__ dneg,
     int tws) {
@@ -618,7 +628,7 @@ constexpr long long kSmallLevelButterflies = 148LL * 128;
 // 5.6 % and 2.5 % slower as pairs, 33 limbs 0.6 % faster).
 template <int L>
 constexpr long long pair_min_fused_threads() {
-  return 148LL * 128 * level_min_blocks<L>();
+  return 148LL * 128 * pair_min_blocks<L>();
 }
 
 // Below this many butterflies a level runs as mp_level_warp_kernel, from 9
