@@ -6,7 +6,8 @@
 // conjugate pair), then one L-shaped butterfly per k in [0, n/4).  Here the
 // same tree is executed breadth-first: one launch runs every leaf (n = 4, 2 or
 // 1), then one launch per node size n = 8, 16, ..., N runs every butterfly of
-// every node of that size.  All nodes of one size are independent, so each
+// every node of that size (for large batches one launch per two node sizes,
+// mp_level_pair_kernel).  All nodes of one size are independent, so each
 // launch is one flat grid over (node, k, signal); consecutive threads are
 // consecutive signals of a batch (or consecutive k for a single signal),
 // which makes every limb-plane access a coalesced 128-byte transaction and,
