@@ -622,14 +622,18 @@ __global__ void __launch_bounds__(kWarpBflyThreads) mp_level_warp_kernel(uint32_
 // per launch) the one-thread-per-butterfly kernel is 1.5x faster.
 constexpr long long kSmallLevelButterflies = 148LL * 128;
 
-// Two levels run as one mp_level_pair_kernel launch when its fused threads
-// (three butterflies each) fill at least one wave of the GPU; with fewer the
-// single-level launches keep more butterflies in flight (N=1024, batch 256,
-// where the top pair has 32768 fused threads: 3, 5, 9 and 17 limbs 4 %, 4.6 %,
-// 5.6 % and 2.5 % slower as pairs, 33 limbs 0.6 % faster).
+// Two levels run as one mp_level_pair_kernel launch when both would run on
+// mp_level_kernel and, below 31 limbs, the pair's fused threads (three
+// butterflies each) fill at least one wave of the GPU; with fewer the
+// single-level launches keep more butterflies in flight there (N=1024, batch
+// 256, where the top pair has 32768 fused threads: 3, 5, 9 and 17 limbs 4 %,
+// 4.6 %, 5.6 % and 2.5 % slower as pairs).  From 31 limbs the pairs win at
+// every such batch (33 limbs, ms per batch, one level per launch / pairs:
+// 128 signals 0.430 / 0.423, 192 0.486 / 0.478, 256 0.619 / 0.564, 384
+// 0.826 / 0.781, 512 1.056 / 0.906).
 template <int L>
 constexpr long long pair_min_fused_threads() {
-  return 148LL * 128 * pair_min_blocks<L>();
+  return L >= 31 ? 0 : 148LL * 128 * pair_min_blocks<L>();
 }
 
 // Below this many butterflies a level runs as mp_level_warp_kernel, from 9
@@ -694,7 +698,8 @@ static cudaError_t run_transform(const MpDeviceTables &T, const uint32_t *in, ui
     const int lthreads = 128;
     const int blocks = (int)((total + lthreads - 1) / lthreads);
     const long long fused = lv + 1 < T.nlevels ? (long long)T.level_count[lv + 1] * (n / 4) * B : 0;
-    if (fused >= pair_min_fused_threads<L>()) {
+    if (fused > 0 && fused >= pair_min_fused_threads<L>() && total >= kSmallLevelButterflies &&
+        (long long)T.level_count[lv + 1] * (n / 2) * B >= kSmallLevelButterflies) {
       // levels lv and lv+1 in one launch; lv+1's timer entry stays 0
       const long long threads = fused + (long long)T.pair_count[lv] * (n / 4) * B;
       timer.begin();
